@@ -1,0 +1,621 @@
+// C ABI of libgkm_b200.so (declarations and contracts in include/gkm.h).
+//
+// One handle = one periodic cube resident on one GPU.  Two state buffers of
+// 5 x nt^3 doubles alternate: the current state W and the accumulator A that
+// the sweeps fill and the z sweep turns into the next state.  dt, t and the
+// step count stay on the device (DevClock), so a step never waits for the
+// host; with use_graphs the whole step is replayed as one CUDA graph per
+// buffer parity.
+#include "gkm.h"
+#include "gkm_internal.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using gkm::DevClock;
+using gkm::FieldConst;
+
+namespace {
+constexpr int kStatsBlocks = 148 * 4;
+
+enum GraphKind { kGraphEulerian = 0, kGraphFull = 1 };
+}  // namespace
+
+struct gkm_handle {
+    gkm_config cfg{};
+    FieldConst fc{};
+    int nseg = 1, seg_len = 1;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    double* buf[2] = {nullptr, nullptr};
+    int parity = 0;
+    DevClock* clock = nullptr;
+    bool state_loaded = false;
+    int dt_fixed_mode = 0;
+    double dt_fixed = 0.0;
+    gkm::SplineGrid grid{};
+    double* tables = nullptr;  // mt | dp | z, each npts+1
+    double denom = 0.0;
+    double* coef[3] = {nullptr, nullptr, nullptr};
+    double* scratch = nullptr;
+    bool splines_valid = false;
+    int64_t np = 0, cap = 0;
+    double* P[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // y, x, z, u, v, w
+    gkm::StatsPartial* partials = nullptr;
+    double* stats_out = nullptr;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int64_t graph_np[2][2] = {{-1, -1}, {-1, -1}};
+    std::string err;
+};
+
+namespace {
+
+gkm_status fail(gkm_handle* h, gkm_status s, const std::string& msg)
+{
+    if (h) h->err = msg;
+    return s;
+}
+
+gkm_status cuda_fail(gkm_handle* h, cudaError_t e, const char* where)
+{
+    std::string m = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return fail(h, e == cudaErrorMemoryAllocation ? GKM_ERR_NOMEM : GKM_ERR_CUDA, m);
+}
+
+#define CK(h, expr)                                         \
+    do {                                                    \
+        cudaError_t e_ = (expr);                            \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #expr); \
+    } while (0)
+
+// Thomas tables of the spline line solves; the same recurrences as the line
+// solver's reference formulation: natural dp_1 = 4, m_i = 1/dp_{i-1},
+// dp_i = 4 - m_i; periodic (Sherman-Morrison with gamma = -4) dp_0 = 8,
+// dp_i = b_i - m_i with b_{N-1} = 4.25, z = B^-1 (-4, 0, .., 0, 1).
+void spline_tables(int N, int periodic, std::vector<double>& mt, std::vector<double>& dp, std::vector<double>& z,
+                   double& denom)
+{
+    mt.assign(N + 1, 0.0);
+    dp.assign(N + 1, 0.0);
+    z.assign(N + 1, 0.0);
+    denom = 0.0;
+    if (!periodic) {
+        dp[1] = 4.0;
+        for (int i = 2; i <= N - 2; i++) {
+            mt[i] = 1.0 / dp[i - 1];
+            dp[i] = 4.0 - mt[i];
+        }
+        return;
+    }
+    dp[0] = 8.0;
+    for (int i = 1; i < N; i++) {
+        mt[i] = 1.0 / dp[i - 1];
+        dp[i] = ((i == N - 1) ? 4.25 : 4.0) - mt[i];
+    }
+    double rp = -4.0;
+    z[0] = rp;
+    for (int i = 1; i < N; i++) {
+        double r = (i == N - 1) ? 1.0 : 0.0;
+        rp = r - mt[i] * rp;
+        z[i] = rp;
+    }
+    z[N - 1] = z[N - 1] / dp[N - 1];
+    for (int i = N - 2; i >= 0; i--) z[i] = (z[i] - z[i + 1]) / dp[i];
+    denom = 1.0 + (z[0] + (-0.25) * z[N - 1]);
+}
+
+gkm::SplineTables device_tables(const gkm_handle* h)
+{
+    const int N1 = h->grid.npts + 1;
+    return gkm::SplineTables{h->tables, h->tables + N1, h->tables + 2 * N1, h->denom};
+}
+
+long long coef_count(const gkm_handle* h)
+{
+    long long M = h->grid.npts + h->grid.pad;
+    return M * M * M;
+}
+
+void destroy_graphs(gkm_handle* h)
+{
+    for (int k = 0; k < 2; k++)
+        for (int p = 0; p < 2; p++) {
+            if (h->graph[k][p]) cudaGraphExecDestroy(h->graph[k][p]);
+            h->graph[k][p] = nullptr;
+            h->graph_np[k][p] = -1;
+        }
+}
+
+// enqueue one Eulerian step on h->stream (no host synchronisation)
+cudaError_t enqueue_eulerian(gkm_handle* h)
+{
+    gkm::SweepArgs a{};
+    a.W = h->buf[h->parity];
+    a.A = h->buf[h->parity ^ 1];
+    a.fc = h->fc;
+    a.clock = h->clock;
+    a.parity = h->parity;
+    a.dt_fixed_mode = h->dt_fixed_mode;
+    a.dt_fixed = h->dt_fixed;
+    a.seg_len = h->seg_len;
+    for (int d = 0; d < 3; d++) {
+        cudaError_t e = gkm::launch_sweep(d, a, h->nseg, h->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return gkm::launch_halo(h->buf[h->parity ^ 1], h->fc, h->clock, 1, h->stream);
+}
+
+cudaError_t enqueue_splines(gkm_handle* h, const double* W)
+{
+    return gkm::launch_spline_build(W, h->fc, h->grid, device_tables(h), h->coef[0], h->coef[1], h->coef[2],
+                                    h->scratch, h->stream);
+}
+
+// the body of Evolve's loop: Eulerian step, splines of the new state, particles
+cudaError_t enqueue_full(gkm_handle* h)
+{
+    cudaError_t e = enqueue_eulerian(h);
+    if (e != cudaSuccess) return e;
+    const double* Wn = h->buf[h->parity ^ 1];
+    if (h->np > 0) {
+        e = enqueue_splines(h, Wn);
+        if (e != cudaSuccess) return e;
+        const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+        e = gkm::launch_particles_heun(c, h->grid, h->clock, h->np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4],
+                                       h->P[5], h->stream);
+    }
+    return e;
+}
+
+gkm_status run_steps(gkm_handle* h, int32_t nsteps, int kind)
+{
+    if (!h) return GKM_ERR_ARG;
+    if (nsteps < 0) return fail(h, GKM_ERR_ARG, "nsteps < 0");
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    for (int s = 0; s < nsteps; s++) {
+        const int p = h->parity;
+        if (h->cfg.use_graphs) {
+            if (!h->graph[kind][p] || h->graph_np[kind][p] != h->np) {
+                if (h->graph[kind][p]) cudaGraphExecDestroy(h->graph[kind][p]);
+                h->graph[kind][p] = nullptr;
+                cudaGraph_t g = nullptr;
+                CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+                cudaError_t e = kind == kGraphFull ? enqueue_full(h) : enqueue_eulerian(h);
+                cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+                if (e != cudaSuccess) return cuda_fail(h, e, "capture step");
+                if (e2 != cudaSuccess) return cuda_fail(h, e2, "cudaStreamEndCapture");
+                e = cudaGraphInstantiate(&h->graph[kind][p], g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+                h->graph_np[kind][p] = h->np;
+            }
+            CK(h, cudaGraphLaunch(h->graph[kind][p], h->stream));
+        } else {
+            cudaError_t e = kind == kGraphFull ? enqueue_full(h) : enqueue_eulerian(h);
+            if (e != cudaSuccess) return cuda_fail(h, e, "step launch");
+        }
+        h->parity ^= 1;
+        // the particle path leaves the splines of the new state built
+        h->splines_valid = (kind == kGraphFull && h->np > 0);
+    }
+    return GKM_OK;
+}
+
+gkm_status reduce_wave(gkm_handle* h)
+{
+    CK(h, cudaMemsetAsync(&h->clock->wave[h->parity], 0, sizeof(unsigned long long), h->stream));
+    CK(h, gkm::launch_wave_reduce(h->buf[h->parity], h->fc, h->clock, h->parity, h->stream));
+    return GKM_OK;
+}
+
+gkm_status read_clock(gkm_handle* h, DevClock* c)
+{
+    CK(h, cudaMemcpyAsync(c, h->clock, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (c->status & 1) return fail(h, GKM_ERR_NONFINITE, "state holds a non-finite value or non-positive density");
+    return GKM_OK;
+}
+
+gkm_status ensure_splines(gkm_handle* h)
+{
+    if (h->splines_valid) return GKM_OK;
+    CK(h, enqueue_splines(h, h->buf[h->parity]));
+    h->splines_valid = true;
+    return GKM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gkm_abi_version(void) { return GKM_ABI_VERSION; }
+
+void gkm_config_default(gkm_config* cfg)
+{
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->cfl = 0.10;
+    cfg->visc_law = GKM_VISC_SUTHERLAND;
+    cfg->spline_mode = GKM_SPLINE_NATURAL_GHOST3;
+    cfg->precision = GKM_PREC_FP64;
+    cfg->device = 0;
+    cfg->use_graphs = 1;
+}
+
+const char* gkm_last_error(const gkm_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int gkm_nt(const gkm_handle* h) { return h ? h->fc.nt : 0; }
+
+gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
+{
+    if (!cfg || !out) return GKM_ERR_ARG;
+    *out = nullptr;
+    const gkm_params& P = cfg->params;
+    if (P.n < 4 || P.n > 2048) return GKM_ERR_CONFIG;
+    if (!(P.gam > 1.0) || !(P.den0 > 0.0) || !(P.p0 > 0.0) || !(P.mu0 >= 0.0) || !(cfg->cfl > 0.0))
+        return GKM_ERR_CONFIG;
+    if (cfg->visc_law < 0 || cfg->visc_law > 1 || cfg->spline_mode < 0 || cfg->spline_mode > 1) return GKM_ERR_CONFIG;
+    if (cfg->precision != GKM_PREC_FP64 || cfg->max_particles < 0) return GKM_ERR_CONFIG;
+    const int K = (int)((5.0 - 3.0 * P.gam) / (P.gam - 1.0));   // src/FlowField.cpp:42
+    if (K < 0) return GKM_ERR_CONFIG;
+
+    gkm_handle* h = new gkm_handle();
+    h->cfg = *cfg;
+    FieldConst& fc = h->fc;
+    fc.n = P.n;
+    fc.nt = P.n + 6;
+    fc.nt3 = (long long)fc.nt * fc.nt * fc.nt;
+    fc.K = K;
+    fc.visc = cfg->visc_law;
+    fc.gam = P.gam;
+    fc.gm1 = P.gam - 1;
+    fc.dx = 2.0 * (std::atan(1.0) * 4.0) / P.n;   // src/FlowField.cpp:46
+    fc.inv_dx = 1 / fc.dx;
+    fc.mu0 = P.mu0;
+    fc.T0 = P.p0 / (287.0 * P.den0);               // src/FlowField.cpp:47
+    fc.cfl = cfg->cfl;
+
+    // segments along the sweep normal: enough CTAs for ~4 waves of 2 CTAs per SM
+    const long long tiles = (long long)((fc.n + gkm::kTB - 1) / gkm::kTB) * ((fc.n + gkm::kTA - 1) / gkm::kTA);
+    long long nseg = (148LL * 2 * 4 + tiles - 1) / tiles;
+    long long maxseg = fc.n / 16 > 1 ? fc.n / 16 : 1;
+    if (nseg > maxseg) nseg = maxseg;
+    if (nseg < 1) nseg = 1;
+    h->seg_len = (int)((fc.n + nseg - 1) / nseg);
+    h->nseg = (int)((fc.n + h->seg_len - 1) / h->seg_len);
+
+    auto bail = [&](cudaError_t e, const char* where) {
+        gkm_status s = cuda_fail(h, e, where);
+        std::fprintf(stderr, "gkm_create: %s\n", h->err.c_str());
+        gkm_destroy(h);
+        return s;
+    };
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) return bail(e, "cudaSetDevice");
+    e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(e, "cudaStreamCreate");
+    h->stream = h->own_stream;
+    for (int b = 0; b < 2; b++) {
+        e = cudaMalloc(&h->buf[b], sizeof(double) * 5 * (size_t)fc.nt3);
+        if (e != cudaSuccess) return bail(e, "cudaMalloc(state)");
+    }
+    e = cudaMalloc(&h->clock, sizeof(DevClock));
+    if (e != cudaSuccess) return bail(e, "cudaMalloc(clock)");
+    e = cudaMemset(h->clock, 0, sizeof(DevClock));
+    if (e != cudaSuccess) return bail(e, "cudaMemset(clock)");
+
+    // splines
+    h->grid.periodic = cfg->spline_mode == GKM_SPLINE_PERIODIC;
+    h->grid.npts = h->grid.periodic ? fc.n : fc.nt;
+    h->grid.pad = h->grid.periodic ? 3 : 2;
+    if (h->grid.periodic) {
+        h->grid.start = 0.5 * fc.dx;
+        h->grid.dinv = 1.0 / fc.dx;
+    } else {
+        // src/Interpolation.cpp:11-26 with sta = 0; spacing (end-start)/(num-1)
+        double s = (0 - 3) * fc.dx + 0.5 * fc.dx;
+        double en = s + (fc.nt - 1) * fc.dx;
+        h->grid.start = s;
+        h->grid.dinv = 1.0 / ((en - s) / (double)(fc.nt - 1));
+    }
+    {
+        std::vector<double> mt, dp, z;
+        spline_tables(h->grid.npts, h->grid.periodic, mt, dp, z, h->denom);
+        const size_t N1 = (size_t)h->grid.npts + 1;
+        e = cudaMalloc(&h->tables, sizeof(double) * 3 * N1);
+        if (e != cudaSuccess) return bail(e, "cudaMalloc(tables)");
+        std::vector<double> all;
+        all.insert(all.end(), mt.begin(), mt.end());
+        all.insert(all.end(), dp.begin(), dp.end());
+        all.insert(all.end(), z.begin(), z.end());
+        e = cudaMemcpy(h->tables, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return bail(e, "cudaMemcpy(tables)");
+    }
+    const long long M = h->grid.npts + h->grid.pad, N = h->grid.npts;
+    for (int c = 0; c < 3; c++) {
+        e = cudaMalloc(&h->coef[c], sizeof(double) * (size_t)(M * M * M));
+        if (e != cudaSuccess) return bail(e, "cudaMalloc(spline coefficients)");
+    }
+    e = cudaMalloc(&h->scratch, sizeof(double) * (size_t)(M * M * N));
+    if (e != cudaSuccess) return bail(e, "cudaMalloc(spline scratch)");
+    // particles
+    h->cap = cfg->max_particles;
+    if (h->cap > 0)
+        for (int c = 0; c < 6; c++) {
+            e = cudaMalloc(&h->P[c], sizeof(double) * (size_t)h->cap);
+            if (e != cudaSuccess) return bail(e, "cudaMalloc(particles)");
+        }
+    e = cudaMalloc(&h->partials, sizeof(gkm::StatsPartial) * kStatsBlocks);
+    if (e != cudaSuccess) return bail(e, "cudaMalloc(stats)");
+    e = cudaMalloc(&h->stats_out, sizeof(double) * 32);
+    if (e != cudaSuccess) return bail(e, "cudaMalloc(stats)");
+    e = gkm::sweep_prepare();
+    if (e != cudaSuccess) return bail(e, "sweep_prepare");
+    *out = h;
+    return GKM_OK;
+}
+
+gkm_status gkm_destroy(gkm_handle* h)
+{
+    if (!h) return GKM_ERR_ARG;
+    if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+    destroy_graphs(h);
+    for (int b = 0; b < 2; b++) cudaFree(h->buf[b]);
+    cudaFree(h->clock);
+    cudaFree(h->tables);
+    for (int c = 0; c < 3; c++) cudaFree(h->coef[c]);
+    cudaFree(h->scratch);
+    for (int c = 0; c < 6; c++) cudaFree(h->P[c]);
+    cudaFree(h->partials);
+    cudaFree(h->stats_out);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return GKM_OK;
+}
+
+gkm_status gkm_upload_state(gkm_handle* h, const double* const W[5])
+{
+    if (!h || !W) return GKM_ERR_ARG;
+    for (int q = 0; q < 5; q++)
+        if (!W[q]) return fail(h, GKM_ERR_ARG, "W[q] is NULL");
+    const size_t bytes = sizeof(double) * (size_t)h->fc.nt3;
+    double* dst = h->buf[h->parity];
+    for (int q = 0; q < 5; q++)
+        CK(h, cudaMemcpyAsync(dst + (size_t)q * h->fc.nt3, W[q], bytes, cudaMemcpyHostToDevice, h->stream));
+    CK(h, gkm::launch_halo(dst, h->fc, h->clock, 0, h->stream));
+    CK(h, cudaMemsetAsync(&h->clock->status, 0, sizeof(int), h->stream));
+    gkm_status s = reduce_wave(h);
+    if (s != GKM_OK) return s;
+    h->state_loaded = true;
+    h->splines_valid = false;
+    return GKM_OK;
+}
+
+gkm_status gkm_download_state(gkm_handle* h, double* const W[5])
+{
+    if (!h || !W) return GKM_ERR_ARG;
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    const size_t bytes = sizeof(double) * (size_t)h->fc.nt3;
+    const double* src = h->buf[h->parity];
+    for (int q = 0; q < 5; q++) {
+        if (!W[q]) return fail(h, GKM_ERR_ARG, "W[q] is NULL");
+        CK(h, cudaMemcpyAsync(W[q], src + (size_t)q * h->fc.nt3, bytes, cudaMemcpyDeviceToHost, h->stream));
+    }
+    DevClock c;
+    return read_clock(h, &c);
+}
+
+gkm_status gkm_timestep(gkm_handle* h, double* dt_out)
+{
+    if (!h) return GKM_ERR_ARG;
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    gkm_status s = reduce_wave(h);
+    if (s != GKM_OK) return s;
+    DevClock c;
+    s = read_clock(h, &c);
+    if (s != GKM_OK) return s;
+    double mw;
+    unsigned long long bits = c.wave[h->parity];
+    std::memcpy(&mw, &bits, sizeof(mw));
+    if (h->dt_fixed_mode) destroy_graphs(h);
+    h->dt_fixed_mode = 0;
+    if (dt_out) *dt_out = h->fc.cfl * h->fc.dx / mw;   // src/update.cpp:1053
+    return GKM_OK;
+}
+
+gkm_status gkm_set_dt(gkm_handle* h, double dt)
+{
+    if (!h) return GKM_ERR_ARG;
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(h, GKM_ERR_ARG, "dt must be >= 0 and finite");
+    h->dt_fixed_mode = dt > 0.0;
+    h->dt_fixed = dt;
+    destroy_graphs(h);
+    return GKM_OK;
+}
+
+gkm_status gkm_evolve_eulerian(gkm_handle* h, int32_t nsteps) { return run_steps(h, nsteps, kGraphEulerian); }
+
+gkm_status gkm_step(gkm_handle* h, int32_t nsteps) { return run_steps(h, nsteps, kGraphFull); }
+
+gkm_status gkm_evolve(gkm_handle* h, double* const W[5], double dt)
+{
+    if (!h || !W) return GKM_ERR_ARG;
+    if (!(dt > 0.0)) return fail(h, GKM_ERR_ARG, "dt must be > 0");
+    gkm_status s = gkm_upload_state(h, (const double* const*)W);
+    if (s != GKM_OK) return s;
+    const int mode = h->dt_fixed_mode;
+    const double val = h->dt_fixed;
+    h->dt_fixed_mode = 1;
+    h->dt_fixed = dt;
+    cudaError_t e = enqueue_eulerian(h);
+    h->dt_fixed_mode = mode;
+    h->dt_fixed = val;
+    if (e != cudaSuccess) return cuda_fail(h, e, "evolve");
+    h->parity ^= 1;
+    h->splines_valid = false;
+    return gkm_download_state(h, W);
+}
+
+gkm_status gkm_get_clock(gkm_handle* h, double* t, double* dt, int64_t* iter)
+{
+    if (!h) return GKM_ERR_ARG;
+    DevClock c;
+    gkm_status s = read_clock(h, &c);
+    if (t) *t = c.t;
+    if (dt) *dt = c.dt;
+    if (iter) *iter = c.iter;
+    return s;
+}
+
+gkm_status gkm_synchronize(gkm_handle* h)
+{
+    if (!h) return GKM_ERR_ARG;
+    CK(h, cudaStreamSynchronize(h->stream));
+    return GKM_OK;
+}
+
+gkm_status gkm_particles_upload(gkm_handle* h, int64_t np, const double* pos, const double* U)
+{
+    if (!h || (np > 0 && !pos)) return GKM_ERR_ARG;
+    if (np < 0 || np > h->cap) return fail(h, GKM_ERR_ARG, "particle count exceeds max_particles");
+    std::vector<double> tmp((size_t)np);
+    for (int c = 0; c < 6; c++) {
+        const double* src = c < 3 ? pos : U;
+        if (!src) continue;
+        for (int64_t p = 0; p < np; p++) tmp[(size_t)p] = src[3 * p + (c % 3)];
+        CK(h, cudaMemcpyAsync(h->P[c], tmp.data(), sizeof(double) * (size_t)np, cudaMemcpyHostToDevice, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
+    h->np = np;
+    if (!U && np > 0) {
+        if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "U == NULL needs an uploaded state");
+        gkm_status s = ensure_splines(h);
+        if (s != GKM_OK) return s;
+        const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+        CK(h, gkm::launch_particles_eval(c, h->grid, np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4], h->P[5],
+                                         h->stream));
+    }
+    return GKM_OK;
+}
+
+gkm_status gkm_particles_download(gkm_handle* h, double* pos, double* U)
+{
+    if (!h) return GKM_ERR_ARG;
+    std::vector<double> tmp((size_t)h->np);
+    for (int c = 0; c < 6; c++) {
+        double* dst = c < 3 ? pos : U;
+        if (!dst) continue;
+        CK(h, cudaMemcpyAsync(tmp.data(), h->P[c], sizeof(double) * (size_t)h->np, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (int64_t p = 0; p < h->np; p++) dst[3 * p + (c % 3)] = tmp[(size_t)p];
+    }
+    DevClock c;
+    return read_clock(h, &c);
+}
+
+gkm_status gkm_generate_splines(gkm_handle* h)
+{
+    if (!h) return GKM_ERR_ARG;
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    h->splines_valid = false;
+    return ensure_splines(h);
+}
+
+gkm_status gkm_spline_coefs(gkm_handle* h, int32_t c, double* out, int64_t capacity)
+{
+    if (!h || !out || c < 0 || c > 2) return GKM_ERR_ARG;
+    if (capacity < coef_count(h)) return fail(h, GKM_ERR_ARG, "capacity below (N+P)^3");
+    gkm_status s = ensure_splines(h);
+    if (s != GKM_OK) return s;
+    CK(h, cudaMemcpyAsync(out, h->coef[c], sizeof(double) * (size_t)coef_count(h), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return GKM_OK;
+}
+
+gkm_status gkm_stats_compute(gkm_handle* h, gkm_stats* out)
+{
+    if (!h || !out) return GKM_ERR_ARG;
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    gkm_status s = ensure_splines(h);
+    if (s != GKM_OK) return s;
+    const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+    CK(h, gkm::launch_stats(h->buf[h->parity], h->fc, h->grid, c, h->partials, kStatsBlocks, h->stats_out, h->stream));
+    double v[32];
+    CK(h, cudaMemcpyAsync(v, h->stats_out, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    DevClock ck;
+    s = read_clock(h, &ck);
+    if (s != GKM_OK) return s;
+    const gkm_params& P = h->cfg.params;
+    const double gam = P.gam, Mt = P.Mt;
+    out->t_over_t0 = ck.t / P.t0;
+    out->TKE = v[0];
+    out->Diss = v[1];
+    out->SijSij = v[2];
+    // src/update.cpp:793-798
+    out->SKEWu = v[4] / std::pow(v[3], 1.5);
+    out->SKEWv = v[7] / std::pow(v[6], 1.5);
+    out->SKEWw = v[10] / std::pow(v[9], 1.5);
+    out->KURTu = v[5] / std::pow(v[3], 2);
+    out->KURTv = v[8] / std::pow(v[6], 2);
+    out->KURTw = v[11] / std::pow(v[9], 2);
+    // src/update.cpp:825-833
+    out->Prms = v[16] / (gam * P.p0 * Mt * Mt);
+    out->Trms = v[17] / ((gam - 1) * h->fc.T0 * Mt * Mt);
+    out->Vrms = v[18] / (Mt * Mt / P.den0);
+    return GKM_OK;
+}
+
+gkm_status gkm_flux_faces(const double* in, int64_t nfaces, double gam, double dt, double dx, double* F)
+{
+    if (nfaces < 0 || (nfaces > 0 && (!in || !F))) return GKM_ERR_ARG;
+    if (nfaces == 0) return GKM_OK;
+    if (!(gam > 1.0)) return GKM_ERR_ARG;
+    const int K = (int)((5.0 - 3.0 * gam) / (gam - 1.0));
+    double *din = nullptr, *dF = nullptr;
+    cudaError_t e = cudaMalloc(&din, sizeof(double) * 51 * (size_t)nfaces);
+    if (e == cudaSuccess) e = cudaMalloc(&dF, sizeof(double) * 5 * (size_t)nfaces);
+    if (e == cudaSuccess) e = cudaMemcpy(din, in, sizeof(double) * 51 * (size_t)nfaces, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = gkm::launch_flux_faces(din, nfaces, gam, K, dt, dx, dF, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(F, dF, sizeof(double) * 5 * (size_t)nfaces, cudaMemcpyDeviceToHost);
+    cudaFree(din);
+    cudaFree(dF);
+    return e == cudaSuccess ? GKM_OK : GKM_ERR_CUDA;
+}
+
+gkm_status gkm_weno_faces(const double* stencils, int64_t n, double gam, double* Wl, double* Wr)
+{
+    if (n < 0 || (n > 0 && (!stencils || !Wl || !Wr))) return GKM_ERR_ARG;
+    if (n == 0) return GKM_OK;
+    double *ds = nullptr, *dl = nullptr, *dr = nullptr;
+    cudaError_t e = cudaMalloc(&ds, sizeof(double) * 30 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&dl, sizeof(double) * 5 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&dr, sizeof(double) * 5 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMemcpy(ds, stencils, sizeof(double) * 30 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = gkm::launch_weno_faces(ds, n, gam, dl, dr, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(Wl, dl, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(Wr, dr, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost);
+    cudaFree(ds);
+    cudaFree(dl);
+    cudaFree(dr);
+    return e == cudaSuccess ? GKM_OK : GKM_ERR_CUDA;
+}
+
+gkm_status gkm_set_stream(gkm_handle* h, void* stream)
+{
+    if (!h) return GKM_ERR_ARG;
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    destroy_graphs(h);
+    return GKM_OK;
+}
+
+gkm_status gkm_device_state(gkm_handle* h, double** W)
+{
+    if (!h || !W) return GKM_ERR_ARG;
+    *W = h->buf[h->parity];
+    return GKM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// Internal declarations shared by the kernel files and the C-ABI layer.
+// Not part of the public interface (include/gkm.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gkm {
+
+// Device-resident clock of one run: the reference keeps dt, t and iter as
+// globals (src/update.cpp:6,10); here they live in device memory so that a
+// step never waits for the host.
+struct DevClock {
+    double dt;                   // dt of the step being taken (written by the x sweep)
+    double t;                    // simulated time after the last completed step
+    long long iter;              // completed steps
+    unsigned long long wave[2];  // max(|u|+c) of the current/next state, as double bits
+    int status;                  // bit 0: non-finite state detected
+    int pad;
+};
+
+// Physical and grid constants of one field (reference globals of src/param.h:11-27).
+struct FieldConst {
+    int n;          // interior cells per side
+    int nt;         // n + 6
+    long long nt3;  // nt^3
+    int K;
+    int visc;       // 0 Sutherland, 1 power law 0.76
+    double gam, gm1, dx, inv_dx, mu0, T0, cfl;
+};
+
+// Sweep geometry: a CTA covers a kTB x kTA window of faces in the plane
+// normal to the sweep and marches along the normal through seg_len faces.
+constexpr int kTB = 16;             // window width along the first in-plane axis (threadIdx.x)
+constexpr int kTA = 8;              // window height along the second in-plane axis (threadIdx.y)
+constexpr int kWB = kTB + 2;        // window incl. one neighbour face each side
+constexpr int kWA = kTA + 2;
+constexpr int kWC = kWA * kWB;      // cells in one slab of the window
+constexpr int kSweepThreads = kTA * kTB;
+constexpr int kRing = 6;            // slabs held: the 6-cell WENO stencil
+constexpr int kSlabComps = 6;       // rho, rho u, rho v, rho w, rho E, T
+constexpr size_t kSweepSmem = sizeof(double) * (size_t)(kRing * kSlabComps * kWC + 10 * kWC);
+
+struct SweepArgs {
+    const double* __restrict__ W;   // current state, 5 components of nt^3 (reference layout)
+    double* __restrict__ A;         // accumulator; the z sweep overwrites it with the new state
+    FieldConst fc;
+    DevClock* clock;
+    int parity;                     // wave slot holding max(|u|+c) of W
+    int dt_fixed_mode;              // 1: use dt_fixed instead of cfl dx / max(|u|+c)
+    double dt_fixed;
+    int seg_len;                    // faces per CTA along the normal
+};
+
+// kernel launchers (sweep.cu); sweep_prepare sets the sweep kernels' shared-memory limit once
+cudaError_t sweep_prepare();
+cudaError_t launch_sweep(int dir, const SweepArgs& a, int nseg, cudaStream_t s);
+cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, cudaStream_t s);
+cudaError_t launch_wave_reduce(const double* W, const FieldConst& fc, DevClock* clock, int slot, cudaStream_t s);
+cudaError_t launch_flux_faces(const double* in, long long nfaces, double gam, int K, double dt, double dx,
+                              double* F, cudaStream_t s);
+cudaError_t launch_weno_faces(const double* stencils, long long n, double gam, double* Wl, double* Wr,
+                              cudaStream_t s);
+
+// Lagrangian side (lagrangian.cu)
+struct SplineGrid {
+    int npts;        // data points per axis
+    int pad;         // 2 natural, 3 periodic
+    int periodic;
+    double start, dinv;
+};
+
+struct SplineTables {
+    const double* mt;    // Thomas multipliers, length npts+1
+    const double* dp;    // Thomas pivots
+    const double* z;     // periodic correction vector (periodic only)
+    double denom;        // periodic Sherman-Morrison denominator
+};
+
+cudaError_t launch_spline_build(const double* W, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
+                                double* coef_u, double* coef_v, double* coef_w, double* scratch, cudaStream_t s);
+cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np,
+                                  const double* py, const double* px, const double* pz,
+                                  double* Uu, double* Uv, double* Uw, cudaStream_t s);
+cudaError_t launch_particles_heun(const double* const coefs[3], const SplineGrid& g, const DevClock* clock,
+                                  long long np, double* py, double* px, double* pz, double* Uu, double* Uv,
+                                  double* Uw, cudaStream_t s);
+
+struct StatsPartial {  // per-CTA partial sums of the PrintStats moments
+    double v[16];
+};
+cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const double* const coefs[3],
+                         StatsPartial* partials, int nblocks, double* out16, cudaStream_t s);
+
+}  // namespace gkm

@@ -1,0 +1,442 @@
+// Device numerics of the gas-kinetic step: WENO-SYMOO reconstruction and the
+// BGK flux integrated over one time step.  Templated on the arithmetic type T
+// (double for the FP64 drop-in, float for the mixed-precision form).
+//
+// Mathematics follow the reference CPU path:
+//   WENO-SYMOO        src/update.cpp:556-680
+//   flux              src/GKMflux.cpp:11-229
+//   moment products   src/GKMflux.cpp:238-278 (MCal)
+//   slope solve       src/GKMflux.cpp:283-297
+//   c2p               src/GKMflux.cpp:302-309
+//
+// The flux is reorganised for registers, not re-derived: every moment product
+// of the reference is formed, but each slope vector is consumed as soon as it
+// is known (its contributions to the tangential/A-slope right-hand sides and
+// to the flux are accumulated at once), so only one side's moment tables are
+// live at a time.  Divisions by per-face constants become multiplications by
+// one reciprocal.  The results differ from the reference only by rounding.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace gkm {
+
+constexpr double kR = 287.0;        // gas constant, src/param.h:21
+constexpr double kPrandtl = 0.70;   // src/param.h:19
+constexpr double kWenoEps = 1e-10;  // pow(10,-10), src/param.h:18
+
+template <class T>
+struct Phys {
+    T gam;        // ratio of specific heats
+    T gm1;        // gam - 1
+    T Rg;         // gas constant in the working units
+    int K;        // internal degrees of freedom (int((5-3g)/(g-1)))
+};
+
+// ---------------------------------------------------------------- WENO ----
+// One scalar, both sides of the face between cells L (=a1) and R (=b1).
+// a3, a2, a1 = cells L-2, L-1, L ; b1, b2, b3 = cells R, R+1, R+2.
+// Linear weights 1/20, 9/20, 9/20, 1/20; IS_3 replaced by max(IS_0..IS_3);
+// alpha_k = g_k / (eps + IS_k).  The normalised weights are formed with one
+// division: w_k = g_k prod_{m!=k}(eps+IS_m) / sum_m g_m prod_{m'!=m}(eps+IS_m').
+template <class T>
+__device__ __forceinline__ void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
+{
+    const T c13 = T(1.0 / 3.0), c76 = T(7.0 / 6.0), c116 = T(11.0 / 6.0), c16 = T(1.0 / 6.0), c56 = T(5.0 / 6.0);
+    const T c1312 = T(13.0 / 12.0), c14 = T(0.25);
+    // candidate polynomials (left-biased "p", right-biased "n")
+    T P0p = a3 * c13 - a2 * c76 + a1 * c116;
+    T P0n = b3 * c13 - b2 * c76 + b1 * c116;
+    T P1p = -a2 * c16 + a1 * c56 + b1 * c13;
+    T P1n = -b2 * c16 + b1 * c56 + a1 * c13;
+    T P2p = a1 * c13 + b1 * c56 - b2 * c16;
+    T P2n = b1 * c13 + a1 * c56 - a2 * c16;
+    T P3p = b1 * c116 - b2 * c76 + b3 * c13;
+    T P3n = a1 * c116 - a2 * c76 + a3 * c13;
+    // smoothness indicators
+    T d;
+    T e;
+    d = a3 - T(2) * a2 + a1; e = a3 - T(4) * a2 + T(3) * a1; T I0p = c1312 * d * d + c14 * e * e;
+    d = b3 - T(2) * b2 + b1; e = b3 - T(4) * b2 + T(3) * b1; T I0n = c1312 * d * d + c14 * e * e;
+    d = a2 - T(2) * a1 + b1; e = b1 - a2;                    T I1p = c1312 * d * d + c14 * e * e;
+    d = b2 - T(2) * b1 + a1; e = a1 - b2;                    T I1n = c1312 * d * d + c14 * e * e;
+    d = a1 - T(2) * b1 + b2; e = -T(3) * a1 + T(4) * b1 - b2; T I2p = c1312 * d * d + c14 * e * e;
+    d = b1 - T(2) * a1 + a2; e = -T(3) * b1 + T(4) * a1 - a2; T I2n = c1312 * d * d + c14 * e * e;
+    d = b1 - T(2) * b2 + b3; e = -T(5) * b1 + T(8) * b2 - T(3) * b3; T I3p = c1312 * d * d + c14 * e * e;
+    d = a1 - T(2) * a2 + a3; e = -T(5) * a1 + T(8) * a2 - T(3) * a3; T I3n = c1312 * d * d + c14 * e * e;
+    I3p = fmax(fmax(fmax(I0p, I1p), I2p), I3p);
+    I3n = fmax(fmax(fmax(I0n, I1n), I2n), I3n);
+    {
+        T e0 = eps + I0p, e1 = eps + I1p, e2 = eps + I2p, e3 = eps + I3p;
+        T p01 = e0 * e1, p23 = e2 * e3;
+        T n0 = e1 * p23, n1 = T(9) * e0 * p23, n2 = T(9) * p01 * e3, n3 = p01 * e2;
+        fl = (n0 * P0p + n1 * P1p + n2 * P2p + n3 * P3p) / (n0 + n1 + n2 + n3);
+    }
+    {
+        T e0 = eps + I0n, e1 = eps + I1n, e2 = eps + I2n, e3 = eps + I3n;
+        T p01 = e0 * e1, p23 = e2 * e3;
+        T n0 = e1 * p23, n1 = T(9) * e0 * p23, n2 = T(9) * p01 * e3, n3 = p01 * e2;
+        fr = (n0 * P0n + n1 * P1n + n2 * P2n + n3 * P3n) / (n0 + n1 + n2 + n3);
+    }
+}
+
+// temperature of a conserved state, src/update.cpp:615-620
+template <class T>
+__device__ __forceinline__ T temperature(T r, T m1, T m2, T m3, T E, const Phys<T>& ph)
+{
+    T ir = T(1) / r;
+    return ph.gm1 * (E * ir - T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) * ir * ir) / ph.Rg;
+}
+
+// face energy from reconstructed rho, momentum and temperature, src/update.cpp:673-674
+template <class T>
+__device__ __forceinline__ T face_energy(T r, T m1, T m2, T m3, T Tf, const Phys<T>& ph)
+{
+    return r * ph.Rg * Tf / ph.gm1 + T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) / r;
+}
+
+// ------------------------------------------------------ moment tables ----
+// Maxwellian moments of one state: x half-space table H (and H2 for the
+// equilibrium state's other half), full tables X (x), Y (y), Z (z).
+// src/GKMflux.cpp:45-68 (l, r) and :85-103 (e).
+template <class T>
+struct Moments {
+    T H[7];
+    T X[7];
+    T Y[6];
+    T Z[6];
+    T Ie2, Ie4;
+};
+
+template <class T>
+__device__ __forceinline__ T erfc_t(T x);
+template <>
+__device__ __forceinline__ double erfc_t<double>(double x) { return erfc(x); }
+template <>
+__device__ __forceinline__ float erfc_t<float>(float x) { return erfcf(x); }
+template <class T>
+__device__ __forceinline__ T exp_t(T x);
+template <>
+__device__ __forceinline__ double exp_t<double>(double x) { return exp(x); }
+template <>
+__device__ __forceinline__ float exp_t<float>(float x) { return expf(x); }
+template <class T>
+__device__ __forceinline__ T sqrt_t(T x);
+template <>
+__device__ __forceinline__ double sqrt_t<double>(double x) { return sqrt(x); }
+template <>
+__device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
+
+// half: +1 positive-u half space (erfc(-sqrt(lam) u)/2), -1 negative half
+template <class T>
+__device__ __forceinline__ void half_table(T* H, T U0, T lam, T inv2lam, int half)
+{
+    const T pi = T(3.14159265358979323846);
+    T sl = sqrt_t<T>(lam);
+    T g = T(0.5) * exp_t<T>(-lam * U0 * U0) / sqrt_t<T>(lam * pi);
+    if (half > 0) {
+        H[0] = T(0.5) * erfc_t<T>(-sl * U0);
+        H[1] = U0 * H[0] + g;
+    } else {
+        H[0] = T(0.5) * erfc_t<T>(sl * U0);
+        H[1] = U0 * H[0] - g;
+    }
+#pragma unroll
+    for (int i = 2; i < 7; i++) H[i] = U0 * H[i - 1] + H[i - 2] * (T(i - 1) * inv2lam);
+}
+
+template <class T, int N>
+__device__ __forceinline__ void full_table(T* F, T U, T inv2lam)
+{
+    F[0] = T(1);
+    F[1] = U;
+#pragma unroll
+    for (int i = 2; i < N; i++) F[i] = U * F[i - 1] + F[i - 2] * (T(i - 1) * inv2lam);
+}
+
+template <class T>
+__device__ __forceinline__ void build_moments(Moments<T>& M, const T U[3], T lam, int K, int half)
+{
+    T inv2lam = T(1) / (T(2) * lam);
+    M.Ie2 = T(K) * inv2lam;
+    M.Ie4 = T(3 * K + K * (K - 1)) * inv2lam * inv2lam;
+    half_table<T>(M.H, U[0], lam, inv2lam, half);
+    full_table<T, 7>(M.X, U[0], inv2lam);
+    full_table<T, 6>(M.Y, U[1], inv2lam);
+    full_table<T, 6>(M.Z, U[2], inv2lam);
+}
+
+// ----------------------------------------------------------- MCal -----
+// <psi (u^k v^l w^m) (a0 + a1 u + a2 v + a3 w + a4 psi4)> with psi = (1,u,v,w,psi4),
+// psi4 = (u^2+v^2+w^2+xi^2)/2; I = normal table (full or half), Y, Z tangential.
+template <int k, int l, int m, class T>
+__device__ __forceinline__ void mcal(T M[5], const T* I, const T* Y, const T* Z, T Ie2, T Ie4, const T a[5])
+{
+#define TM(A, B, C) (I[k + (A)] * Y[l + (B)] * Z[m + (C)])
+    T t000 = TM(0, 0, 0), t100 = TM(1, 0, 0), t010 = TM(0, 1, 0), t001 = TM(0, 0, 1);
+    T t200 = TM(2, 0, 0), t020 = TM(0, 2, 0), t002 = TM(0, 0, 2);
+    T t110 = TM(1, 1, 0), t101 = TM(1, 0, 1), t011 = TM(0, 1, 1);
+    T v0 = T(0.5) * (t200 + t020 + t002 + t000 * Ie2);
+    T v1 = T(0.5) * (TM(3, 0, 0) + TM(1, 2, 0) + TM(1, 0, 2) + t100 * Ie2);
+    T v2 = T(0.5) * (TM(2, 1, 0) + TM(0, 3, 0) + TM(0, 1, 2) + t010 * Ie2);
+    T v3 = T(0.5) * (TM(2, 0, 1) + TM(0, 2, 1) + TM(0, 0, 3) + t001 * Ie2);
+    M[0] = a[0] * t000 + a[1] * t100 + a[2] * t010 + a[3] * t001 + a[4] * v0;
+    M[1] = a[0] * t100 + a[1] * t200 + a[2] * t110 + a[3] * t101 + a[4] * v1;
+    M[2] = a[0] * t010 + a[1] * t110 + a[2] * t020 + a[3] * t011 + a[4] * v2;
+    M[3] = a[0] * t001 + a[1] * t101 + a[2] * t011 + a[3] * t002 + a[4] * v3;
+    M[4] = T(0.25) * a[4] *
+               (TM(4, 0, 0) + TM(0, 4, 0) + TM(0, 0, 4) + t000 * Ie4 +
+                T(2) * (TM(2, 2, 0) + TM(2, 0, 2) + t200 * Ie2 + TM(0, 2, 2) + t020 * Ie2 + t002 * Ie2)) +
+           a[0] * v0 + a[1] * v1 + a[2] * v2 + a[3] * v3;
+#undef TM
+}
+
+template <int k, int l, int m, class T>
+__device__ __forceinline__ void mcal0(T M[5], const T* I, const T* Y, const T* Z, T Ie2)
+{
+#define TM(A, B, C) (I[k + (A)] * Y[l + (B)] * Z[m + (C)])
+    M[0] = TM(0, 0, 0);
+    M[1] = TM(1, 0, 0);
+    M[2] = TM(0, 1, 0);
+    M[3] = TM(0, 0, 1);
+    M[4] = T(0.5) * (TM(2, 0, 0) + TM(0, 2, 0) + TM(0, 0, 2) + TM(0, 0, 0) * Ie2);
+#undef TM
+}
+
+template <class T>
+__device__ __forceinline__ void axpy5(T* acc, T s, const T* M)
+{
+#pragma unroll
+    for (int q = 0; q < 5; q++) acc[q] += s * M[q];
+}
+
+// ----------------------------------------------------- slope solver ---
+// Solve the 5x5 moment system for the Maxwellian slope coefficients, with the
+// Prandtl-number correction on the energy component (src/GKMflux.cpp:283-297).
+template <class T>
+struct SlopeState {
+    T U[3];
+    T lam2;     // 2 lam
+    T usqc;     // u.u + (K+3)/(2 lam)
+    T a4fac;    // (1/Pr) (4 lam^2) / (K+3)
+};
+
+template <class T>
+__device__ __forceinline__ SlopeState<T> slope_state(const T U[3], T lam, int K)
+{
+    SlopeState<T> s;
+    s.U[0] = U[0];
+    s.U[1] = U[1];
+    s.U[2] = U[2];
+    s.lam2 = T(2) * lam;
+    s.usqc = U[0] * U[0] + U[1] * U[1] + U[2] * U[2] + T(K + 3) / s.lam2;
+    s.a4fac = T(1.0 / kPrandtl) * (T(4) * lam * lam) / T(K + 3);
+    return s;
+}
+
+template <class T>
+__device__ __forceinline__ void slope_solve(const T b[5], const SlopeState<T>& s, T a[5])
+{
+    T r2 = b[1] - s.U[0] * b[0];
+    T r3 = b[2] - s.U[1] * b[0];
+    T r4 = b[3] - s.U[2] * b[0];
+    T r5 = T(2) * b[4] - b[0] * s.usqc;
+    a[4] = s.a4fac * (r5 - T(2) * (s.U[0] * r2 + s.U[1] * r3 + s.U[2] * r4));
+    a[3] = s.lam2 * r4 - s.U[2] * a[4];
+    a[2] = s.lam2 * r3 - s.U[1] * a[4];
+    a[1] = s.lam2 * r2 - s.U[0] * a[4];
+    a[0] = b[0] - a[1] * s.U[0] - a[2] * s.U[1] - a[3] * s.U[2] - T(0.5) * a[4] * s.usqc;
+}
+
+template <class T>
+__device__ __forceinline__ void c2p(const T W[5], T gm1, T& den, T U[3], T& P)
+{
+    den = W[0];
+    T ir = T(1) / den;
+    U[0] = W[1] * ir;
+    U[1] = W[2] * ir;
+    U[2] = W[3] * ir;
+    P = (den * gm1) * (W[4] * ir - T(0.5) * (U[0] * U[0] + U[1] * U[1] + U[2] * U[2]));
+}
+
+// --------------------------------------------------------- the flux ----
+// The face inputs come from a provider so that the 30 slope values are formed
+// where they are consumed instead of being held in registers.  A provider has
+//   T WL(int q), WR(int q)   cell averages left/right of the face
+//   T Wl(int q), Wr(int q)   reconstructed face states
+//   T DW(int v, int q)       slope vectors v = 0..5: DWxl, DWxr, DWyl, DWyr, DWzl, DWzr
+// all in the face frame (slot 1 = normal momentum).  tau0 = mu(T_L)/p_L of the
+// left cell.  Output F[5] = flux integrated over [0, dt] (not divided by dt).
+template <class T>
+struct FaceInput {
+    T WL_[5], WR_[5], Wl_[5], Wr_[5];
+    T DW_[6][5];
+    __device__ T WL(int q) const { return WL_[q]; }
+    __device__ T WR(int q) const { return WR_[q]; }
+    __device__ T Wl(int q) const { return Wl_[q]; }
+    __device__ T Wr(int q) const { return Wr_[q]; }
+    __device__ T DW(int v, int q) const { return DW_[v][q]; }
+};
+
+template <class T, class Prov>
+__device__ __forceinline__ void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[5])
+{
+    const int K = ph.K;
+    T denl, Ul[3], Pl, denr, Ur[3], Pr;
+    {
+        T wl[5], wr[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            wl[q] = in.Wl(q);
+            wr[q] = in.Wr(q);
+        }
+        c2p<T>(wl, ph.gm1, denl, Ul, Pl);
+        c2p<T>(wr, ph.gm1, denr, Ur, Pr);
+    }
+    T laml = T(0.5) * denl / Pl;
+    T lamr = T(0.5) * denr / Pr;
+
+    // collision time with the pressure-jump correction, src/GKMflux.cpp:156-157
+    T ql = denl / laml, qr = denr / lamr;
+    T tau = tau0 + dt * (fabs(ql - qr) / fabs(ql + qr));
+    T ex = exp_t<T>(-dt / tau);
+    T omx = T(1) - ex;
+    // time coefficients, src/GKMflux.cpp:162-167,197-204
+    T gm0 = dt - tau * omx;
+    T igm0 = T(1) / gm0;
+    T gm1 = -omx * igm0;
+    T gm2 = (-dt + T(2) * tau * omx - dt * ex) * igm0;
+    T gm3 = -gm1;
+    T gm4 = (dt * ex - tau * omx) * igm0;
+    T gm5 = tau * gm3;
+    T Pc = tau * omx;                               // -tau (e - 1)
+    T Qc = -tau * dt * ex + tau * tau * omx;        // -tau dt e - tau^2 (e - 1)
+    T p0 = dt - Pc;
+    T p1 = T(0.5) * dt * dt - tau * p0;
+    T p2 = -tau * p0 + Qc;
+    T p3 = Pc;
+    T p4 = -Qc - tau * Pc;
+    T p5 = -tau * Pc;
+
+    T We[5] = {0, 0, 0, 0, 0};      // equilibrium state at the face, src/GKMflux.cpp:73-77
+    T by_[5] = {0, 0, 0, 0, 0}, bz_[5] = {0, 0, 0, 0, 0};
+    T Bacc[5] = {0, 0, 0, 0, 0};   // B_ * dene, without the gm1/gm3 terms
+    T Facc[5] = {0, 0, 0, 0, 0};
+    T M[5];
+
+    const T cB = gm4 + gm5;
+    // ---------------- one side (l: positive half with left state, r: negative half with right state)
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+        const T den = side == 0 ? denl : denr;
+        const T* Us = side == 0 ? Ul : Ur;
+        const T lam = side == 0 ? laml : lamr;
+        Moments<T> S;
+        build_moments<T>(S, Us, lam, K, side == 0 ? +1 : -1);
+        SlopeState<T> ss = slope_state<T>(Us, lam, K);
+        T iden = T(1) / den;
+        mcal0<0, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2);
+        axpy5<T>(We, den, M);
+        T Bs[5] = {0, 0, 0, 0, 0};   // -(Mf100 ax + Mf010 ay + Mf001 az)
+        T b[5], a[5];
+        // normal slope
+#pragma unroll
+        for (int q = 0; q < 5; q++) b[q] = in.DW(0 + side, q) * iden;
+        slope_solve<T>(b, ss, a);
+        mcal<1, 0, 0, T>(M, S.X, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Bs, T(-1), M);
+        mcal<1, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Bacc, cB * den, M);
+        mcal<2, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Facc, p4 * den, M);
+        // first tangential slope
+#pragma unroll
+        for (int q = 0; q < 5; q++) b[q] = in.DW(2 + side, q) * iden;
+        slope_solve<T>(b, ss, a);
+        mcal<0, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(by_, T(1), M);
+        mcal<0, 1, 0, T>(M, S.X, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Bs, T(-1), M);
+        mcal<0, 1, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Bacc, cB * den, M);
+        mcal<1, 1, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Facc, p4 * den, M);
+        // second tangential slope
+#pragma unroll
+        for (int q = 0; q < 5; q++) b[q] = in.DW(4 + side, q) * iden;
+        slope_solve<T>(b, ss, a);
+        mcal<0, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(bz_, T(1), M);
+        mcal<0, 0, 1, T>(M, S.X, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Bs, T(-1), M);
+        mcal<0, 0, 1, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Bacc, cB * den, M);
+        mcal<1, 0, 1, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Facc, p4 * den, M);
+        // time slope of this side, src/GKMflux.cpp:145-151
+        slope_solve<T>(Bs, ss, a);
+        mcal<0, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Bacc, gm5 * den, M);
+        mcal<1, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        axpy5<T>(Facc, p5 * den, M);
+        // free transport of the initial half-Maxwellian
+        mcal0<1, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2);
+        axpy5<T>(Facc, p3 * den, M);
+    }
+
+    // ---------------- equilibrium part
+    T dene, Ue[3], Pe;
+    c2p<T>(We, ph.gm1, dene, Ue, Pe);
+    T lame = T(0.5) * dene / Pe;
+    Moments<T> E;
+    build_moments<T>(E, Ue, lame, K, +1);
+    T H2[7];
+    {
+        T inv2lam = T(1) / (T(2) * lame);
+        half_table<T>(H2, Ue[0], lame, inv2lam, -1);
+    }
+    SlopeState<T> se = slope_state<T>(Ue, lame, K);
+    T b[5], a[5];
+    const T idx2 = T(2) / (dene * dx);
+    // normal equilibrium slopes from the cell averages, src/GKMflux.cpp:115-116
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (We[q] - in.WL(q)) * idx2;
+    slope_solve<T>(b, se, a);
+    mcal<1, 0, 0, T>(M, E.H, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    mcal<2, 0, 0, T>(M, E.H, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Facc, p2 * dene, M);
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (in.WR(q) - We[q]) * idx2;
+    slope_solve<T>(b, se, a);
+    mcal<1, 0, 0, T>(M, H2, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    mcal<2, 0, 0, T>(M, H2, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Facc, p2 * dene, M);
+    // tangential equilibrium slopes
+    slope_solve<T>(by_, se, a);
+    mcal<0, 1, 0, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    mcal<1, 1, 0, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Facc, p2 * dene, M);
+    slope_solve<T>(bz_, se, a);
+    mcal<0, 0, 1, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    mcal<1, 0, 1, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Facc, p2 * dene, M);
+    // time derivative of the equilibrium, src/GKMflux.cpp:183-191
+    mcal0<0, 0, 0, T>(M, E.X, E.Y, E.Z, E.Ie2);
+    T idene = T(1) / dene;
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (gm1 * dene * M[q] + Bacc[q] + gm3 * We[q]) * idene;
+    slope_solve<T>(b, se, a);
+    mcal<1, 0, 0, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    axpy5<T>(Facc, p1 * dene, M);
+    mcal0<1, 0, 0, T>(M, E.X, E.Y, E.Z, E.Ie2);
+    axpy5<T>(Facc, p0 * dene, M);
+#pragma unroll
+    for (int q = 0; q < 5; q++) F[q] = Facc[q];
+}
+
+}  // namespace gkm

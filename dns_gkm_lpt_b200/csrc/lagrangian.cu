@@ -1,0 +1,418 @@
+// Lagrangian side of the step on sm_100a: velocity splines, tricubic
+// evaluation, Heun advection and the PrintStats reductions.
+//
+// Reference path replaced: generateSplines (src/update.cpp:1235-1247) ->
+// get_bsplinep (src/Interpolation.cpp:3-31) -> einspline; Particle::
+// updatePosition / track (src/ParticleTrack.cpp:42-73); the velocity part of
+// getParticleProp (:99-113); PrintStats (src/update.cpp:688-842).
+//
+// Splines are uniform cubic B-splines built as batched 1-D line solves along
+// each axis (axis 0 = y first, then x, then z).  Two end conditions:
+//   natural_ghost3: the reference's grid (nt points from -3dx+dx/2, f''=0 at
+//                   both ends), coefficients c_{-1}..c_{N} (N+2 per axis);
+//   periodic:       the n interior cell centres, cyclic rows, stored N+3 per
+//                   axis with wrapped copies so a 4-point window never wraps.
+// The line solve and the evaluation use rounding-explicit intrinsics in the
+// order of the CPU oracle, so both produce the same bits.
+#include "gkm_internal.h"
+
+namespace gkm {
+namespace {
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+// One line: f (N points, stride fs) -> c (N+pad values, stride cs).
+template <class Src>
+__device__ void line_solve(const Src& f, int N, int periodic, const SplineTables& tb, double* c, long long cs)
+{
+    if (!periodic) {
+        const double c0 = f(0), cl = f(N - 1);
+        double rp = 0.0;
+        for (int i = 1; i <= N - 2; i++) {
+            double r = mul(6.0, f(i));
+            if (i == 1) r = sub(r, c0);
+            if (i == N - 2) r = sub(r, cl);
+            rp = (i == 1) ? r : sub(r, mul(tb.mt[i], rp));
+            c[(long long)(i + 1) * cs] = rp;
+        }
+        double x = __ddiv_rn(c[(long long)(N - 1) * cs], tb.dp[N - 2]);
+        c[(long long)(N - 1) * cs] = x;
+        for (int i = N - 3; i >= 1; i--) {
+            x = __ddiv_rn(sub(c[(long long)(i + 1) * cs], x), tb.dp[i]);
+            c[(long long)(i + 1) * cs] = x;
+        }
+        // x now holds c_1 (or c_{N-2} when N == 3)
+        const double x1 = (N - 2 >= 1) ? c[2 * cs] : cl;
+        const double xl2 = (N - 2 >= 1) ? c[(long long)(N - 1) * cs] : c0;
+        c[cs] = c0;
+        c[(long long)N * cs] = cl;
+        c[0] = sub(2.0 * c0, x1);
+        c[(long long)(N + 1) * cs] = sub(2.0 * cl, xl2);
+    } else {
+        // y = B^-1 (6 f) stored in slots 1..N
+        double rp = mul(6.0, f(0));
+        c[cs] = rp;
+        for (int i = 1; i < N; i++) {
+            rp = sub(mul(6.0, f(i)), mul(tb.mt[i], rp));
+            c[(long long)(i + 1) * cs] = rp;
+        }
+        double x = __ddiv_rn(c[(long long)N * cs], tb.dp[N - 1]);
+        c[(long long)N * cs] = x;
+        for (int i = N - 2; i >= 0; i--) {
+            x = __ddiv_rn(sub(c[(long long)(i + 1) * cs], x), tb.dp[i]);
+            c[(long long)(i + 1) * cs] = x;
+        }
+        const double fac = __ddiv_rn(add(c[cs], mul(-0.25, c[(long long)N * cs])), tb.denom);
+        for (int i = 0; i < N; i++) c[(long long)(i + 1) * cs] = sub(c[(long long)(i + 1) * cs], mul(fac, tb.z[i]));
+        c[0] = c[(long long)N * cs];
+        c[(long long)(N + 1) * cs] = c[cs];
+        c[(long long)(N + 2) * cs] = c[2 * cs];
+    }
+}
+
+// pass 0: velocity component q of W along axis 0 (y) -> out [M0][N1][N2]
+__global__ void spline_pass0(const double* __restrict__ W, FieldConst fc, SplineGrid g, SplineTables tb, int q,
+                             double* __restrict__ out)
+{
+    const int N = g.npts;
+    const long long lines = (long long)N * N;
+    const long long nt3 = fc.nt3;
+    const int nt = fc.nt;
+    const int off = g.periodic ? 3 : 0;
+    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(L / N), k = (int)(L - (long long)i * N);
+        const long long base = (long long)(i + off) * nt + (k + off);
+        const long long sj = (long long)nt * nt;
+        auto f = [&](int j) {
+            const long long idx = (long long)(j + off) * sj + base;
+            return __ddiv_rn(W[q * nt3 + idx], W[idx]);   // u = rho u / rho, src/update.cpp:1239-1241
+        };
+        line_solve(f, N, g.periodic, tb, out + L, lines);
+    }
+}
+
+// pass 1: [M0][N1][N2] along axis 1 -> [M0][M1][N2]
+__global__ void spline_pass1(const double* __restrict__ in, SplineGrid g, SplineTables tb, double* __restrict__ out)
+{
+    const int N = g.npts, M = N + g.pad;
+    const long long lines = (long long)M * N;
+    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(L / N), k = (int)(L - (long long)a * N);
+        const double* src = in + (long long)a * N * N + k;
+        auto f = [&](int i) { return src[(long long)i * N]; };
+        line_solve(f, N, g.periodic, tb, out + (long long)a * M * N + k, N);
+    }
+}
+
+// pass 2: [M0][M1][N2] along axis 2 -> [M0][M1][M2]
+__global__ void spline_pass2(const double* __restrict__ in, SplineGrid g, SplineTables tb, double* __restrict__ out)
+{
+    const int N = g.npts, M = N + g.pad;
+    const long long lines = (long long)M * M;
+    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x) {
+        const double* src = in + L * N;
+        auto f = [&](int k) { return src[k]; };
+        line_solve(f, N, g.periodic, tb, out + L * M, 1);
+    }
+}
+
+struct Basis {
+    double w[4];
+};
+
+__device__ __forceinline__ int locate(const SplineGrid& g, double x, double& t)
+{
+    const double u = mul(sub(x, g.start), g.dinv);
+    const double fl = floor(u);
+    int i = (int)fl;
+    if (g.periodic) {
+        t = sub(u, fl);
+        i %= g.npts;
+        if (i < 0) i += g.npts;
+        return i;
+    }
+    if (i < 0) i = 0;
+    if (i > g.npts - 2) i = g.npts - 2;
+    t = sub(u, (double)i);
+    return i;
+}
+
+__device__ __forceinline__ Basis basis(double t)
+{
+    const double t2 = mul(t, t), t3 = mul(t2, t), s = sub(1.0, t);
+    const double c = 1.0 / 6.0;
+    Basis b;
+    b.w[0] = mul(c, mul(mul(s, s), s));
+    b.w[1] = mul(c, add(sub(mul(3.0, t3), mul(6.0, t2)), 4.0));
+    b.w[2] = mul(c, add(add(add(mul(-3.0, t3), mul(3.0, t2)), mul(3.0, t)), 1.0));
+    b.w[3] = mul(c, t3);
+    return b;
+}
+
+// value of one spline at a point (the oracle's contraction order: z, then x, then y)
+__device__ __forceinline__ double spline_value(const double* __restrict__ C, const SplineGrid& g, int ia, int ib, int ic,
+                                               const Basis& A, const Basis& B, const Basis& Cz)
+{
+    const long long M = g.npts + g.pad;
+    double v = 0.0;
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        double bw = 0.0;
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const double* row = C + ((long long)(ia + x) * M + (ib + y)) * M + ic;
+            const double cw = add(add(add(mul(Cz.w[0], row[0]), mul(Cz.w[1], row[1])), mul(Cz.w[2], row[2])),
+                                  mul(Cz.w[3], row[3]));
+            bw = (y == 0) ? mul(B.w[0], cw) : add(bw, mul(B.w[y], cw));
+        }
+        v = add(v, mul(A.w[x], bw));
+    }
+    return v;
+}
+
+__device__ __forceinline__ void eval3(const double* const* coefs, const SplineGrid& g, double a, double b, double c,
+                                      double out[3])
+{
+    double ta, tb, tc;
+    const int ia = locate(g, a, ta), ib = locate(g, b, tb), ic = locate(g, c, tc);
+    const Basis A = basis(ta), B = basis(tb), Cz = basis(tc);
+#pragma unroll
+    for (int f = 0; f < 3; f++) out[f] = spline_value(coefs[f], g, ia, ib, ic, A, B, Cz);
+}
+
+struct Coefs3 {
+    const double* c[3];
+};
+
+__global__ void particles_eval_kernel(Coefs3 cf, SplineGrid g, long long np, const double* __restrict__ py,
+                                      const double* __restrict__ px, const double* __restrict__ pz,
+                                      double* __restrict__ Uu, double* __restrict__ Uv, double* __restrict__ Uw)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        double U[3];
+        eval3(cf.c, g, py[p], px[p], pz[p], U);
+        Uu[p] = U[0];
+        Uv[p] = U[1];
+        Uw[p] = U[2];
+    }
+}
+
+// Heun step (src/ParticleTrack.cpp:48-73): U from the previous evaluation,
+// U2 from the new spline at pos + U dt (pos is (y, x, z), U is (u, v, w)),
+// pos += (U + U2) dt / 2, periodic wrap, then U at the new position for the
+// next step's predictor (the reference's getParticleProp at loop start).
+__global__ void particles_heun_kernel(Coefs3 cf, SplineGrid g, const DevClock* __restrict__ clock, long long np,
+                                      double* __restrict__ py, double* __restrict__ px, double* __restrict__ pz,
+                                      double* __restrict__ Uu, double* __restrict__ Uv, double* __restrict__ Uw)
+{
+    const double dt = clock->dt;
+    const double twopi = 2.0 * 3.14159265358979311600;   // 2 * atan(1)*4 in double
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        double pos[3] = {py[p], px[p], pz[p]};
+        const double U[3] = {Uu[p], Uv[p], Uw[p]};
+        double U2[3];
+        eval3(cf.c, g, add(pos[0], mul(U[1], dt)), add(pos[1], mul(U[0], dt)), add(pos[2], mul(U[2], dt)), U2);
+        pos[0] = add(pos[0], mul(mul(0.5, add(U[1], U2[1])), dt));
+        pos[1] = add(pos[1], mul(mul(0.5, add(U[0], U2[0])), dt));
+        pos[2] = add(pos[2], mul(mul(0.5, add(U[2], U2[2])), dt));
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            if (pos[q] > twopi) pos[q] = fmod(pos[q], twopi);
+            if (pos[q] < 0) pos[q] = sub(twopi, fmod(-pos[q], twopi));
+        }
+        double Un[3];
+        eval3(cf.c, g, pos[0], pos[1], pos[2], Un);
+        py[p] = pos[0];
+        px[p] = pos[1];
+        pz[p] = pos[2];
+        Uu[p] = Un[0];
+        Uv[p] = Un[1];
+        Uw[p] = Un[2];
+    }
+}
+
+// ---------------------------------------------------------------- stats --
+// PrintStats (src/update.cpp:688-842) on the device.  At a node the spline
+// value equals the data (interpolation), so rho and u come from the cell; the
+// gradients come from the coefficients: per axis the node weights are
+// (1, 4, 1)/6 for values and (-1, 0, 1)/2 * dinv for the derivative.
+__device__ __forceinline__ void node_grad(const double* __restrict__ C, long long M, int a, int b, int c, double dinv,
+                                          double g[3])
+{
+    const double w[3] = {1.0 / 6.0, 4.0 / 6.0, 1.0 / 6.0};
+    const double d[3] = {-0.5 * dinv, 0.0, 0.5 * dinv};
+    double g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+    for (int x = 0; x < 3; x++)
+#pragma unroll
+        for (int y = 0; y < 3; y++) {
+            const double* row = C + ((long long)(a + x) * M + (b + y)) * M + c;
+            const double cw = w[0] * row[0] + w[1] * row[1] + w[2] * row[2];
+            const double cd = d[0] * row[0] + d[2] * row[2];
+            g0 += d[x] * w[y] * cw;
+            g1 += w[x] * d[y] * cw;
+            g2 += w[x] * w[y] * cd;
+        }
+    g[0] = g0;
+    g[1] = g1;
+    g[2] = g2;
+}
+
+__device__ __forceinline__ double visc(const FieldConst& fc, double T)
+{
+    double x = T / fc.T0;
+    if (fc.visc == 1) return fc.mu0 * pow(x, 0.76);
+    return fc.mu0 * pow(x, 1.5) * (fc.T0 + 110.4) / (T + 110.4);
+}
+
+__device__ __forceinline__ void cell_c2p(const double* W, long long nt3, long long idx, double gm1, double& d, double& u,
+                                         double& v, double& w, double& P, double& T)
+{
+    d = W[idx];
+    u = W[nt3 + idx] / d;
+    v = W[2 * nt3 + idx] / d;
+    w = W[3 * nt3 + idx] / d;
+    const double vs = u * u + v * v + w * w;
+    P = (d * gm1) * (W[4 * nt3 + idx] / d - 0.5 * vs);
+    T = P / (287.0 * d);
+}
+
+template <int PASS>
+__global__ void stats_kernel(const double* __restrict__ W, FieldConst fc, SplineGrid g, Coefs3 cf,
+                             const double* __restrict__ means, StatsPartial* __restrict__ part)
+{
+    __shared__ double red[16][32];
+    const int n = fc.n, nt = fc.nt;
+    const long long nt3 = fc.nt3, total = (long long)n * n * n;
+    const long long M = g.npts + g.pad;
+    const int off = g.periodic ? 0 : 3;   // coefficient window start of interior cell m
+    double acc[16];
+#pragma unroll
+    for (int s = 0; s < 16; s++) acc[s] = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(e / ((long long)n * n)), i = (int)((e / n) % n), k = (int)(e % n);
+        const long long idx = ((long long)(j + 3) * nt + (i + 3)) * nt + (k + 3);
+        double d, u, v, w, P, T;
+        cell_c2p(W, nt3, idx, fc.gm1, d, u, v, w, P, T);
+        if (PASS == 0) {
+            double gu[3], gv[3], gw[3];
+            node_grad(cf.c[0], M, j + off, i + off, k + off, g.dinv, gu);
+            node_grad(cf.c[1], M, j + off, i + off, k + off, g.dinv, gv);
+            node_grad(cf.c[2], M, j + off, i + off, k + off, g.dinv, gw);
+            const double dudx = gu[1], dudy = gu[0], dudz = gu[2];
+            const double dvdx = gv[1], dvdy = gv[0], dvdz = gv[2];
+            const double dwdx = gw[1], dwdy = gw[0], dwdz = gw[2];
+            const double a2 = dudx * dudx + dudy * dudy + dudz * dudz + dvdx * dvdx + dvdy * dvdy + dvdz * dvdz +
+                              dwdx * dwdx + dwdy * dwdy + dwdz * dwdz;
+            acc[0] += d * (u * u + v * v + w * w);                      // TKE
+            acc[1] += visc(fc, T) * a2;                                 // Diss
+            acc[2] += dudx * dudx + 0.5 * (dudy + dvdx) * (dudy + dvdx) + 0.5 * (dudz + dwdx) * (dudz + dwdx) +
+                      0.5 * (dwdy + dvdz) * (dwdy + dvdz) + dvdy * dvdy + dwdz * dwdz;   // SijSij
+            acc[3] += dudx * dudx;
+            acc[4] += dudx * dudx * dudx;
+            acc[5] += dudx * dudx * dudx * dudx;
+            acc[6] += dvdy * dvdy;
+            acc[7] += dvdy * dvdy * dvdy;
+            acc[8] += dvdy * dvdy * dvdy * dvdy;
+            acc[9] += dwdz * dwdz;
+            acc[10] += dwdz * dwdz * dwdz;
+            acc[11] += dwdz * dwdz * dwdz * dwdz;
+            acc[12] += P;
+            acc[13] += T;
+            acc[14] += 1.0 / d;
+        } else {
+            acc[0] += (means[0] - P) * (means[0] - P);
+            acc[1] += (means[1] - T) * (means[1] - T);
+            acc[2] += (means[2] - 1.0 / d) * (means[2] - 1.0 / d);
+        }
+    }
+    // deterministic block reduction: warp shuffles, then warp partials in fixed order
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < 16; s++) {
+        double v = acc[s];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[s][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 16) {
+        double v = 0.0;
+        for (int w2 = 0; w2 < (int)(blockDim.x >> 5); w2++) v += red[threadIdx.x][w2];
+        part[blockIdx.x].v[threadIdx.x] = v;
+    }
+}
+
+// sums partials in block order (deterministic); PASS 0 also forms the means for pass 1
+__global__ void stats_finish(const StatsPartial* __restrict__ part, int nblocks, double ncells, int pass,
+                             double* __restrict__ out)
+{
+    const int s = threadIdx.x;
+    if (s >= 16) return;
+    double v = 0.0;
+    for (int b = 0; b < nblocks; b++) v += part[b].v[s];
+    if (pass == 0) out[s] = v / ncells;
+    else if (s < 3) out[16 + s] = sqrt(v / ncells);
+}
+
+template <class K, class... Args>
+cudaError_t grid_launch(K kernel, long long work, int threads, cudaStream_t s, Args... args)
+{
+    long long b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    kernel<<<(unsigned)b, threads, 0, s>>>(args...);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_spline_build(const double* W, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
+                                double* coef_u, double* coef_v, double* coef_w, double* scratch, cudaStream_t s)
+{
+    double* outs[3] = {coef_u, coef_v, coef_w};
+    const long long N = g.npts, M = N + g.pad;
+    for (int f = 0; f < 3; f++) {
+        cudaError_t e = grid_launch(spline_pass0, N * N, 128, s, W, fc, g, tb, f + 1, outs[f]);
+        if (e != cudaSuccess) return e;
+        e = grid_launch(spline_pass1, M * N, 128, s, (const double*)outs[f], g, tb, scratch);
+        if (e != cudaSuccess) return e;
+        e = grid_launch(spline_pass2, M * M, 128, s, (const double*)scratch, g, tb, outs[f]);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np, const double* py,
+                                  const double* px, const double* pz, double* Uu, double* Uv, double* Uw,
+                                  cudaStream_t s)
+{
+    if (np <= 0) return cudaSuccess;
+    Coefs3 cf{{coefs[0], coefs[1], coefs[2]}};
+    return grid_launch(particles_eval_kernel, np, 128, s, cf, g, np, py, px, pz, Uu, Uv, Uw);
+}
+
+cudaError_t launch_particles_heun(const double* const coefs[3], const SplineGrid& g, const DevClock* clock, long long np,
+                                  double* py, double* px, double* pz, double* Uu, double* Uv, double* Uw,
+                                  cudaStream_t s)
+{
+    if (np <= 0) return cudaSuccess;
+    Coefs3 cf{{coefs[0], coefs[1], coefs[2]}};
+    return grid_launch(particles_heun_kernel, np, 128, s, cf, g, clock, np, py, px, pz, Uu, Uv, Uw);
+}
+
+cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const double* const coefs[3],
+                         StatsPartial* partials, int nblocks, double* out, cudaStream_t s)
+{
+    Coefs3 cf{{coefs[0], coefs[1], coefs[2]}};
+    const double ncells = (double)fc.n * fc.n * fc.n;
+    stats_kernel<0><<<nblocks, 256, 0, s>>>(W, fc, g, cf, nullptr, partials);
+    stats_finish<<<1, 32, 0, s>>>(partials, nblocks, ncells, 0, out);
+    // means of p, T, 1/rho sit in out[12..14]
+    stats_kernel<1><<<nblocks, 256, 0, s>>>(W, fc, g, cf, out + 12, partials);
+    stats_finish<<<1, 32, 0, s>>>(partials, nblocks, ncells, 1, out);
+    return cudaGetLastError();
+}
+
+}  // namespace gkm

@@ -1,0 +1,182 @@
+"""Python host mirror of the reference's interface for the hot path.
+
+The reference drives the step from C++ globals and free functions
+(src/update.h:14-81, src/FlowField.h, src/ParticleTrack.h); ``Solver`` keeps
+those names and argument meanings on top of the C ABI (include/gkm.h):
+
+    reference                                   Solver
+    GetParams / segment / MAKE5s / DevAlloc     Solver(params, cfl, ...)
+    Initialize_DHIT(W)                          upload_state(W)
+    evolve(W, dev, dt)            GPUupdate.h   evolve(W, dt)          (host arrays in/out)
+    evolveEulerian + HaloTransfer update.cpp    evolve_eulerian(nsteps)
+    timestep(W)                                 timestep()
+    generateSplines (u, v, w)                   generate_splines()
+    locateParticles / getParticleProp           particles_upload(pos, U=None)
+    Evolve's loop body                          step(nsteps)
+    PrintStats                                  print_stats()
+
+Arrays follow the reference layout: W is (5, nt, nt, nt) float64 in (y, x, z)
+order with 3 ghost layers; particle positions are (np, 3) as (y, x, z).
+Errors raise GkmError carrying the gkm_status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from .ic import Params
+
+_dp = C.POINTER(C.c_double)
+
+
+class GkmError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_capi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _w5(W: np.ndarray):
+    if W.dtype != np.float64 or not W.flags.c_contiguous or W.ndim != 4 or W.shape[0] != 5:
+        raise ValueError("W must be a C-contiguous float64 array of shape (5, nt, nt, nt)")
+    return (_dp * 5)(*[_ptr(W[q]) for q in range(5)])
+
+
+class Solver:
+    def __init__(self, params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
+                 max_particles: int = 0, device: int = 0, use_graphs: bool = True):
+        self.L = _capi.lib()
+        cfg = _capi.GkmConfig()
+        self.L.gkm_config_default(C.byref(cfg))
+        cfg.params = _capi.GkmParams(n=params.n, gam=params.gam, den0=params.den0, Mt=params.Mt, Re=params.Re,
+                                     mu0=params.mu0, p0=params.p0, t0=params.t0)
+        cfg.cfl = cfl
+        cfg.visc_law = visc_law
+        cfg.spline_mode = spline_mode
+        cfg.device = device
+        cfg.max_particles = max_particles
+        cfg.use_graphs = 1 if use_graphs else 0
+        h = C.c_void_p()
+        s = self.L.gkm_create(C.byref(cfg), C.byref(h))
+        if s != 0:
+            raise GkmError(s, "gkm_create failed (see stderr)")
+        self.h = h
+        self.params = params
+        self.n = params.n
+        self.nt = self.L.gkm_nt(h)
+        self.spline_mode = spline_mode
+        self.np = 0
+
+    # -- plumbing ----------------------------------------------------------
+    def _check(self, s: int) -> None:
+        if s != 0:
+            raise GkmError(s, self.L.gkm_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.gkm_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- field ---------------------------------------------------------------
+    def upload_state(self, W: np.ndarray) -> None:
+        self._check(self.L.gkm_upload_state(self.h, _w5(W)))
+
+    def download_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty((5, self.nt, self.nt, self.nt)) if out is None else out
+        self._check(self.L.gkm_download_state(self.h, _w5(out)))
+        return out
+
+    def timestep(self) -> float:
+        dt = C.c_double()
+        self._check(self.L.gkm_timestep(self.h, C.byref(dt)))
+        return dt.value
+
+    def set_dt(self, dt: float) -> None:
+        self._check(self.L.gkm_set_dt(self.h, dt))
+
+    def evolve_eulerian(self, nsteps: int = 1) -> None:
+        self._check(self.L.gkm_evolve_eulerian(self.h, nsteps))
+
+    def evolve(self, W: np.ndarray, dt: float) -> None:
+        """The reference GPU plug point evolve(W, dev, dt): W updated in place."""
+        self._check(self.L.gkm_evolve(self.h, _w5(W), dt))
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self.L.gkm_step(self.h, nsteps))
+
+    def clock(self):
+        t, dt, it = C.c_double(), C.c_double(), C.c_int64()
+        self._check(self.L.gkm_get_clock(self.h, C.byref(t), C.byref(dt), C.byref(it)))
+        return t.value, dt.value, it.value
+
+    def synchronize(self) -> None:
+        self._check(self.L.gkm_synchronize(self.h))
+
+    # -- particles -------------------------------------------------------------
+    def particles_upload(self, pos_yxz: np.ndarray, U: np.ndarray | None = None) -> None:
+        pos = np.ascontiguousarray(pos_yxz, dtype=np.float64)
+        Up = None if U is None else _ptr(np.ascontiguousarray(U, dtype=np.float64))
+        self._check(self.L.gkm_particles_upload(self.h, len(pos), _ptr(pos) if len(pos) else None, Up))
+        self.np = len(pos)
+
+    def particles_download(self):
+        pos = np.empty((self.np, 3))
+        U = np.empty((self.np, 3))
+        self._check(self.L.gkm_particles_download(self.h, _ptr(pos), _ptr(U)))
+        return pos, U
+
+    # -- splines / stats -------------------------------------------------------
+    def generate_splines(self) -> None:
+        self._check(self.L.gkm_generate_splines(self.h))
+
+    def spline_coefs(self, c: int) -> np.ndarray:
+        N = self.nt if self.spline_mode == 0 else self.n
+        M = N + (2 if self.spline_mode == 0 else 3)
+        out = np.empty((M, M, M))
+        self._check(self.L.gkm_spline_coefs(self.h, c, _ptr(out), out.size))
+        return out
+
+    def print_stats(self) -> dict:
+        st = _capi.GkmStats()
+        self._check(self.L.gkm_stats_compute(self.h, C.byref(st)))
+        return st.as_dict()
+
+
+def flux_faces(inputs: np.ndarray, gam: float, dt: float, dx: float) -> np.ndarray:
+    """flux() on independent faces: inputs (nf, 51) = WL WR Wl Wr DW[6x5] tau."""
+    L = _capi.lib()
+    a = np.ascontiguousarray(inputs, dtype=np.float64)
+    F = np.zeros((len(a), 5))
+    s = L.gkm_flux_faces(_ptr(a), len(a), gam, dt, dx, _ptr(F))
+    if s != 0:
+        raise GkmError(s, "gkm_flux_faces")
+    return F
+
+
+def weno_faces(stencils: np.ndarray, gam: float):
+    """ApplyWENO on stencils (n, 6, 5) -> (Wl, Wr) each (n, 5)."""
+    L = _capi.lib()
+    a = np.ascontiguousarray(stencils, dtype=np.float64)
+    Wl = np.zeros((len(a), 5))
+    Wr = np.zeros((len(a), 5))
+    s = L.gkm_weno_faces(_ptr(a), len(a), gam, _ptr(Wl), _ptr(Wr))
+    if s != 0:
+        raise GkmError(s, "gkm_weno_faces")
+    return Wl, Wr

@@ -1,0 +1,190 @@
+/*
+ * gkm.h — C ABI of the B200-native DNS_GKM_LPT step (libgkm_b200.so).
+ *
+ * Drop-in boundary for the reference's hot path: the compressible
+ * decaying-isotropic-turbulence step (WENO-SYMOO reconstruction, gas-kinetic
+ * flux, conservative update, dt / TKE / dissipation reductions) and the
+ * Lagrangian-particle step (velocity splines, tricubic evaluation, Heun
+ * advection) of nishantp9/DNS_GKM_LPT.  Plain pointers and sizes only.
+ *
+ * Data layout at this boundary is the reference's own (src/param.h:26,40-41):
+ * five FP64 arrays W[q], q = rho, rho u, rho v, rho w, rho E, each of
+ * nt^3 = (n+6)^3 values, index (j*nt + i)*nt + k with j = y, i = x, k = z
+ * (z fastest), three ghost layers on each side.  Particle positions are
+ * (y, x, z) and velocities (u, v, w) per particle, as in class Particle
+ * (src/ParticleTrack.h:14-36).
+ *
+ * Every call returns gkm_status; GKM_OK is 0.  Nothing calls exit().  A handle
+ * owns all its device memory and one CUDA stream; host arrays stay owned by
+ * the caller and are touched only inside the call that receives them.  A
+ * handle is not thread-safe; independent handles are.
+ */
+#ifndef GKM_B200_H
+#define GKM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GKM_ABI_VERSION 1
+
+typedef enum gkm_status {
+    GKM_OK = 0,
+    GKM_ERR_ARG = 1,        /* a null pointer, a size out of range, an unknown enum */
+    GKM_ERR_CONFIG = 2,     /* the configuration is not supported */
+    GKM_ERR_CUDA = 3,       /* a CUDA call failed; gkm_last_error() has the text */
+    GKM_ERR_NONFINITE = 4,  /* the state holds NaN/Inf or non-positive density */
+    GKM_ERR_STATE = 5,      /* call out of order (e.g. step before upload) */
+    GKM_ERR_NOMEM = 6       /* device allocation failed */
+} gkm_status;
+
+typedef enum gkm_visc_law {
+    GKM_VISC_SUTHERLAND = 0, /* mu0 (T/T0)^1.5 (T0+110.4)/(T+110.4), src/update.cpp:277 */
+    GKM_VISC_POWER076 = 1    /* mu0 (T/T0)^0.76 */
+} gkm_visc_law;
+
+typedef enum gkm_spline_mode {
+    GKM_SPLINE_NATURAL_GHOST3 = 0, /* the reference's grid: nt points, natural ends (src/Interpolation.cpp:3-31) */
+    GKM_SPLINE_PERIODIC = 1        /* n interior cell centres, periodic */
+} gkm_spline_mode;
+
+typedef enum gkm_precision {
+    GKM_PREC_FP64 = 0 /* FP64 everywhere (the reference's ptype = double) */
+} gkm_precision;
+
+/* Contents of InitialConditions/params, read by GetParams (src/FlowField.cpp:9-58). */
+typedef struct gkm_params {
+    int32_t n;      /* cells per side (nc) */
+    int32_t pad_;
+    double gam;     /* ratio of specific heats */
+    double den0;    /* reference density */
+    double Mt;      /* turbulent Mach number */
+    double Re;      /* Taylor Reynolds number */
+    double mu0;     /* reference viscosity */
+    double p0;      /* reference pressure */
+    double t0;      /* eddy turnover time */
+} gkm_params;
+
+typedef struct gkm_config {
+    gkm_params params;
+    double cfl;              /* the reference fixes 0.10 at compile time (src/param.h:20) */
+    int32_t visc_law;        /* gkm_visc_law */
+    int32_t spline_mode;     /* gkm_spline_mode */
+    int32_t precision;       /* gkm_precision */
+    int32_t device;          /* CUDA device ordinal */
+    int64_t max_particles;   /* capacity of the particle arrays */
+    int32_t use_graphs;      /* 1: replay each step as a captured CUDA graph */
+    int32_t reserved[7];
+} gkm_config;
+
+/* One PrintStats line (src/update.cpp:835-840), field part. */
+typedef struct gkm_stats {
+    double t_over_t0, TKE, Diss, SijSij;
+    double SKEWu, SKEWv, SKEWw, KURTu, KURTv, KURTw;
+    double Prms, Trms, Vrms;
+} gkm_stats;
+
+typedef struct gkm_handle gkm_handle;
+
+/* ---------------------------------------------------------------- life cycle */
+
+/* Defaults: cfl 0.10, Sutherland, natural_ghost3, FP64, device 0, graphs on. */
+void gkm_config_default(gkm_config* cfg);
+
+/* Replaces GetParams + segment + MAKE5s + DevAlloc::DevAlloc
+ * (src/FlowField.cpp:9-58,275-284; src/Main.cpp:36; src/GPUAlloc.cu:3-68)
+ * for a single-GPU run with the whole periodic cube on one device. */
+gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out);
+/* Releases everything the handle owns (DevAlloc::~DevAlloc, src/GPUAlloc.cu:70-132). */
+gkm_status gkm_destroy(gkm_handle* h);
+/* Text of the last error on this handle (never NULL). */
+const char* gkm_last_error(const gkm_handle* h);
+int gkm_abi_version(void);
+/* Cells per side including ghosts (nt = n + 6), the extent of every W array. */
+int gkm_nt(const gkm_handle* h);
+
+/* ------------------------------------------------------------- field state */
+
+/* Host -> device copy of the conserved state in the reference layout, then
+ * the periodic ghost wrap and the dt reduction.  Replaces the H2D half of
+ * evolve() (src/GPUupdate.cu:89-93) and Initialize_DHIT's result
+ * (src/FlowField.cpp:60-114).  Ghost values in W may be stale. */
+gkm_status gkm_upload_state(gkm_handle* h, const double* const W[5]);
+/* Device -> host copy (ghosts included, already wrapped); D2H half of evolve()
+ * (src/GPUupdate.cu:209-213). */
+gkm_status gkm_download_state(gkm_handle* h, double* const W[5]);
+
+/* timestep(W) (src/update.cpp:1031-1054): dt = cfl*dx / max(|u| + c) of the
+ * current state; also makes that dt the one the next step uses. */
+gkm_status gkm_timestep(gkm_handle* h, double* dt_out);
+/* Fix dt for the following steps (dt > 0) or return to the CFL rule (dt == 0). */
+gkm_status gkm_set_dt(gkm_handle* h, double dt);
+
+/* nsteps x { evolveEulerian; HaloTransfer; timestep }
+ * (src/update.cpp:147,154,167; derivsX/Y/Z + update, :206-516).  Asynchronous
+ * on the handle's stream. */
+gkm_status gkm_evolve_eulerian(gkm_handle* h, int32_t nsteps);
+
+/* The reference's GPU plug point, void evolve(ptype *W[5], DevAlloc *dev,
+ * ptype dt) (src/GPUupdate.h:33, src/GPUupdate.cu:79-219): copy W in, take
+ * one Eulerian step with the given dt, copy W out.  Synchronous.  The output
+ * ghosts are already wrapped. */
+gkm_status gkm_evolve(gkm_handle* h, double* const W[5], double dt);
+
+/* nsteps of the body of Evolve's loop (src/update.cpp:124-170): Eulerian
+ * step, velocity splines of the new state (generateSplines, :1235-1247),
+ * particle advection (evolveParticles / Particle::track, :1056-1086 and
+ * src/ParticleTrack.cpp:42-73), dt of the next step.  Asynchronous. */
+gkm_status gkm_step(gkm_handle* h, int32_t nsteps);
+
+/* t, dt of the last step and completed steps (the globals t, dt, iter of
+ * src/update.cpp:6,10).  Synchronises; GKM_ERR_NONFINITE if the state broke. */
+gkm_status gkm_get_clock(gkm_handle* h, double* t, double* dt, int64_t* iter);
+gkm_status gkm_synchronize(gkm_handle* h);
+
+/* -------------------------------------------------------------- particles */
+
+/* Load particles (Particle::initializeParticle / locateParticles,
+ * src/ParticleTrack.cpp:11-17, src/update.cpp:1286-1322); pos is np x (y, x, z).
+ * U (np x (u, v, w)) may be NULL: then U is evaluated from the velocity spline
+ * of the current state (getParticleProp, src/ParticleTrack.cpp:99-107). */
+gkm_status gkm_particles_upload(gkm_handle* h, int64_t np, const double* pos, const double* U);
+gkm_status gkm_particles_download(gkm_handle* h, double* pos, double* U);
+
+/* ---------------------------------------------------------- splines, stats */
+
+/* Build the u, v, w splines of the current state (generateSplines 3-field
+ * form, src/update.cpp:1235-1247, via get_bsplinep, src/Interpolation.cpp:3-31). */
+gkm_status gkm_generate_splines(gkm_handle* h);
+/* Coefficients of velocity component c (0 u, 1 v, 2 w): (N+P)^3 values,
+ * N = nt (natural_ghost3, P = 2) or n (periodic, P = 3); axis 0 slowest. */
+gkm_status gkm_spline_coefs(gkm_handle* h, int32_t c, double* out, int64_t capacity);
+/* PrintStats field moments (src/update.cpp:688-842) of the current state. */
+gkm_status gkm_stats_compute(gkm_handle* h, gkm_stats* out);
+
+/* ---------------------------------------------------- single-call numerics */
+
+/* flux() of src/GKMflux.cpp:11-229 on nfaces independent faces, host
+ * buffers.  in: nfaces x 51 doubles = WL[5] WR[5] Wl[5] Wr[5] DWxl DWxr DWyl
+ * DWyr DWzl DWzr [6x5] tau; F: nfaces x 5.  K = int((5-3gam)/(gam-1)). */
+gkm_status gkm_flux_faces(const double* in, int64_t nfaces, double gam, double dt, double dx, double* F);
+/* ApplyWENO of src/update.cpp:556-680 on n stencils of 6 cells x 5
+ * components (host buffers); Wl, Wr: n x 5. */
+gkm_status gkm_weno_faces(const double* stencils, int64_t n, double gam, double* Wl, double* Wr);
+
+/* ---------------------------------------------------------------- interop */
+
+/* Run on a caller's stream (cudaStream_t passed as void*); NULL restores the
+ * handle's own stream.  Captured step graphs are rebuilt on the next step. */
+gkm_status gkm_set_stream(gkm_handle* h, void* stream);
+/* Device pointer of the current state (5 x nt^3 doubles, component-major);
+ * valid until the next step. */
+gkm_status gkm_device_state(gkm_handle* h, double** W);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,175 @@
+"""Parity of the CUDA path (libgkm_b200.so through the C ABI) with the
+reference's CPU build (golden vectors) and with the CPU oracle.
+
+Tolerances (FP64 drop-in):
+  * fields after 1 and 10 steps: relative L2 per conserved component <= 1e-12
+    (the north-star bar); the CUDA path rounds differently (reciprocals, FMA,
+    reorganised moment sums) but computes the same algorithm;
+  * single-face flux: |dF| <= 1e-11 * max|F| of the face; WENO faces 1e-13 relative;
+  * spline coefficients: bit-exact with the oracle (same rounding order);
+  * particle cell indices: exact; positions 1e-10 absolute (they live in [0, 2 pi));
+  * PrintStats moments: 1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+from dns_gkm_lpt_b200 import ic
+from dns_gkm_lpt_b200.solver import GkmError, Solver, flux_faces, weno_faces
+from tests.gpu_helpers import case, params_of, rel_l2, w0_of
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-12
+
+
+def test_weno_faces_match_reference(golden):
+    f = golden["faces"]
+    Wl, Wr = weno_faces(f["stencils"], float(f["gam"]))
+    for got, ref in ((Wl, f["Wl"]), (Wr, f["Wr"])):
+        scale = np.abs(ref).max(axis=1, keepdims=True)
+        assert np.all(np.abs(got - ref) <= 1e-13 * np.maximum(np.abs(ref), 1e-3 * scale))
+
+
+def test_flux_faces_match_reference(golden):
+    f = golden["faces"]
+    nf = len(f["F"])
+    inp = np.concatenate([f["WL"], f["WR"], f["Wl"], f["Wr"], f["DW"].reshape(nf, 30), f["tau"][:, None]], axis=1)
+    F = flux_faces(inp, float(f["gam"]), float(f["dt"]), float(f["dx"]))
+    err = np.abs(F - f["F"]).max(axis=1) / np.abs(f["F"]).max(axis=1)
+    assert err.max() <= 1e-11, err.max()
+
+
+@pytest.mark.parametrize("name", ["field_16", "field_12"])
+def test_field_and_particles_match_reference(golden, name):
+    g = golden[name]
+    P, W0 = w0_of(g)
+    pos0 = ic.particles_to_reference_order(g["particles_xyz"])
+    with Solver(P, cfl=float(g["cfl"]), max_particles=len(pos0)) as s:
+        s.upload_state(W0)
+        s.particles_upload(pos0)
+        s.step(1)
+        assert rel_l2(s.download_state(), g["W_step1"]).max() <= FIELD_TOL
+        s.step(len(g["dt"]) - 1)
+        W = s.download_state()
+        assert rel_l2(W, g["W_final"]).max() <= FIELD_TOL
+        t, dt_last, it = s.clock()
+        assert it == len(g["dt"])
+        assert dt_last == pytest.approx(g["dt"][-1], rel=1e-13)
+        assert t == pytest.approx(g["dt"].sum(), rel=1e-13)
+        assert s.timestep() == pytest.approx(float(g["dt_next"]), rel=1e-13)
+        pos, U = s.particles_download()
+    order = np.argsort(g["tags"])
+    ref_pos, ref_U = g["pos_final"][order], g["U_final"][order]
+    dx = P.dx
+    assert np.array_equal(np.floor(pos / dx).astype(int), np.floor(ref_pos / dx).astype(int))
+    assert np.abs(pos - ref_pos).max() <= 1e-10
+    assert np.abs(U - ref_U).max() <= 1e-10 * np.abs(ref_U).max()
+
+
+def test_stats_match_reference(golden):
+    g = golden["field_16"]
+    P, W0 = w0_of(g)
+    ref = g["stats_step0"]
+    with Solver(P, cfl=float(g["cfl"])) as s:
+        s.upload_state(W0)
+        st = s.print_stats()
+    for k, i in (("TKE", 1), ("Diss", 2), ("SijSij", 3), ("SKEWu", 4), ("SKEWv", 5), ("SKEWw", 6),
+                 ("KURTu", 7), ("KURTv", 8), ("KURTw", 9)):
+        assert st[k] == pytest.approx(ref[i], rel=1e-10), k
+    assert st["Prms"] == pytest.approx(ref[10], rel=1e-8, abs=1e-12)
+    assert st["Trms"] == pytest.approx(ref[11], rel=1e-8, abs=1e-12)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_spline_coefficients_bitexact_with_oracle(oracle, golden, mode):
+    g = golden["field_12"]
+    P, W0 = w0_of(g)
+    p = oracle.params(P, 0.5)
+    start, dinv = oracle.grid(p, mode)
+    data = W0[1] / W0[0]
+    if mode == 1:
+        data = np.ascontiguousarray(data[3:-3, 3:-3, 3:-3])
+    _, ref = oracle.spline3d(data, mode, start, dinv)
+    with Solver(P, cfl=0.5, spline_mode=mode) as s:
+        s.upload_state(W0)
+        s.generate_splines()
+        got = s.spline_coefs(0)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_particles_match_oracle_both_spline_modes(oracle, mode):
+    P, W0 = case(16, 0.4, 40.0, 31)
+    pos0 = ic.particles_to_reference_order(ic.make_particles(200, 31))
+    p = oracle.params(P, 0.4)
+    Wo = W0.copy()
+    r = oracle.run(p, Wo, 6, mode, pos0, stats=False)
+    with Solver(P, cfl=0.4, spline_mode=mode, max_particles=200) as s:
+        s.upload_state(W0)
+        s.particles_upload(pos0)
+        s.step(6)
+        pos, U = s.particles_download()
+        assert rel_l2(s.download_state(), Wo).max() <= FIELD_TOL
+    assert np.array_equal(np.floor(pos / P.dx), np.floor(r["pos"] / P.dx))
+    assert np.abs(pos - r["pos"]).max() <= 1e-10
+
+
+def test_64cube_step_matches_oracle(oracle):
+    P, W0 = case(64, 0.3, 30.0, 5)
+    p = oracle.params(P, 0.5)
+    Wo = W0.copy()
+    dt = oracle.timestep(p, Wo)
+    oracle.step(p, Wo, dt)
+    with Solver(P, cfl=0.5) as s:
+        s.upload_state(W0)
+        assert s.timestep() == dt
+        s.evolve_eulerian(1)
+        assert rel_l2(s.download_state(), Wo).max() <= FIELD_TOL
+
+
+def test_plug_point_evolve_matches_eulerian_step():
+    P, W0 = case(24, 0.3, 30.0, 8)
+    with Solver(P, cfl=0.5) as s:
+        s.upload_state(W0)
+        dt = s.timestep()
+        s.evolve_eulerian(1)
+        Wa = s.download_state()
+        Wb = W0.copy()
+        s.evolve(Wb, dt)
+    assert np.array_equal(Wa, Wb)
+
+
+def test_graph_replay_is_bitwise_equal_to_direct_launches():
+    P, W0 = case(32, 0.3, 30.0, 9)
+    pos0 = ic.particles_to_reference_order(ic.make_particles(500, 9))
+    out = []
+    for graphs in (True, False):
+        with Solver(P, cfl=0.5, max_particles=500, use_graphs=graphs) as s:
+            s.upload_state(W0)
+            s.particles_upload(pos0)
+            s.step(3)
+            out.append((s.download_state(), s.particles_download()[0]))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_uniform_flow_stays_uniform():
+    n = 32
+    P = ic.Params(n=n, gam=1.4, den0=1.0, Mt=0.3, Re=30.0, mu0=1.0, p0=86100.0, t0=0.01)
+    sh = (n, n, n)
+    W0 = ic.embed_ghost(ic.primitive_to_conserved(P, np.full(sh, 100.0), np.full(sh, -50.0), np.full(sh, 30.0),
+                                                  np.ones(sh), np.full(sh, 86100.0)))
+    with Solver(P, cfl=0.5) as s:
+        s.upload_state(W0)
+        s.evolve_eulerian(3)
+        W = s.download_state()
+    assert rel_l2(W, W0).max() <= 1e-14
+
+
+def test_nonfinite_state_is_reported_not_faulted():
+    P, W0 = case(16, 0.3, 30.0, 3)
+    W0[0, 10, 10, 10] = -1.0   # negative density: sqrt of a negative pressure, a NaN wave speed
+    with Solver(P, cfl=0.5) as s:
+        s.upload_state(W0)
+        with pytest.raises(GkmError) as e:
+            s.timestep()
+        assert e.value.status == 4
