@@ -1,0 +1,300 @@
+"""Benchmark of the DNS_GKM_LPT hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = the body of the reference's Evolve loop on a 256^3 periodic cube
+(FP64, Mt 0.3, Re_lambda 60, cfl 0.5) with 10^6 Lagrangian particles: x/y/z
+fused WENO + gas-kinetic sweeps, halo wrap, dt reduction, velocity splines,
+Heun advection.  The state stays resident in HBM; "value" is Gcell-updates/s
+of the Eulerian step (n^3 x steps / its device time), "particle_steps_per_s"
+the particle part.  "e2e" runs the reference's GPU plug point evolve(W, dt)
+through the C ABI with pinned host buffers: H2D of W, one step, D2H of W,
+every step.
+
+N > 1 (torchrun): each rank advances its own independent replica (the path
+does not shard: no inter-GPU exchange); value sums all ranks over the slowest
+rank's time.
+
+--impl reference: the reference's own CPU code (oracle/_ref, compiled from
+the reference sources) on the host cores, one 64^3 cube per process, all
+processes concurrent, each timed step one reference step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELLS = 256
+N_PART = 1_000_000
+MT, RE, CFL, SEED = 0.3, 60.0, 0.5, 1234
+REF_N = 64                   # reference CPU sample: one 64^3 cube per process
+REF_PART = N_PART * REF_N ** 3 // N_CELLS ** 3   # same particle density
+HBM_PEAK_GBS = 6550.7        # measured copy bandwidth of this pool's B200s
+# DRAM bytes per cell of one sweep launch, from the ncu capture of a 128^3 case (traffic scales with
+# the cells a launch processes; mean over the x, y, z sweeps)
+SWEEP_DRAM_BYTES_PER_CELL = 102.8   # profiles/sweep_kernel_fp64_128cube_full.md, mean of x/y/z
+
+
+def workload(n=N_CELLS, npart=N_PART):
+    return {"workload": f"{n}^3 periodic cube, FP64 drop-in, Mt {MT}, Re_lambda {RE:g}, {npart} particles, "
+                        f"cfl {CFL}, natural_ghost3 splines",
+            "n": n, "particles": npart, "cfl": CFL, "precision": "fp64", "seed": SEED,
+            "l2": "no flush: resident state 2 x 1.44 GB and splines 0.44 GB exceed the 126 MB L2",
+            "parallelism": "replicas"}
+
+
+# ----------------------------------------------------------------- clocks --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------- reference arm ----
+def _ref_worker(args):
+    """One process: the reference CPU build on one seeded REF_N^3 cube."""
+    n, npart, seed, warm, steps = args
+    sys.path.insert(0, ROOT)
+    from dns_gkm_lpt_b200 import ic
+    from oracle import oracle as O
+    d = tempfile.mkdtemp(prefix="gkm_ref_")
+    P, u, v, w, rho, p = ic.make_field(n, MT, RE, seed)
+    ic.write_reference_inputs(d, P, u, v, w, rho, p, ic.make_particles(npart, seed))
+    ref = O.ReferenceRun(d, CFL, True)
+    if warm:
+        ref.time_steps(warm)
+    return [ref.time_steps(1) for _ in range(steps)]
+
+
+def run_reference(workers: int, warm: int, steps: int, n=REF_N, npart=REF_PART):
+    ctx = mp.get_context("spawn")
+    t0 = time.time()
+    with ctx.Pool(workers) as pool:
+        res = pool.map(_ref_worker, [(n, npart, SEED + 17 * w, warm, steps) for w in range(workers)])
+    wall = time.time() - t0
+    te = [sum(s[0] for s in r) for r in res]   # Eulerian seconds per worker
+    tp = [sum(s[1] for s in r) for r in res]   # particle seconds per worker
+    gcell = sum(n ** 3 * steps / t for t in te) / 1e9
+    psteps = sum(npart * steps / t for t in tp) if all(t > 0 for t in tp) else None
+    ms_step = 1e3 * statistics.mean([(a + b) / steps for a, b in zip(te, tp)])
+    return {"gcell": gcell, "psteps": psteps, "ms_per_step": ms_step, "workers": workers, "wall_s": wall}
+
+
+def reference_arm(args, world: int):
+    ncpu = os.cpu_count() or 1
+    workers = max(1, min(ncpu, 96))
+    r = run_reference(workers, args.warmup, args.steps)
+    sample = (f"{REF_N}^3 cube per process (same spectrum recipe, Mt {MT}, Re_lambda {RE:g}), {REF_PART} particles "
+              f"per process, {workers} concurrent processes, each timed step one reference step")
+    line = {"impl": "reference", "metric": "Gcell-updates/s", "value": r["gcell"], "unit": "Gcell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded solenoidal field (init_DNS recipe), uniform particles",
+            "config": workload(), "particle_steps_per_s": r["psteps"],
+            "cpu_baseline": {"value": r["gcell"], "unit": "Gcell-updates/s", "cores": workers, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": r["gcell"], "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- our arm ----
+def ours(args, rank: int, world: int, local_rank: int):
+    import numpy as np
+    import torch
+
+    from dns_gkm_lpt_b200 import ic, opcount
+    from dns_gkm_lpt_b200.solver import Solver, probe_fma_peak
+
+    torch.cuda.set_device(local_rank)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+    n, npart = args.n, args.particles
+    P, u, v, w, rho, p = ic.make_field(n, MT, RE, SEED + rank)
+    W0 = ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, p))
+    del u, v, w, rho, p
+    pos0 = ic.particles_to_reference_order(ic.make_particles(npart, SEED + rank))
+
+    fp64_peak, fp32_peak = probe_fma_peak(local_rank)
+    stream = torch.cuda.Stream()
+    s = Solver(P, cfl=CFL, max_particles=npart, device=local_rank)
+    s.set_stream(stream.cuda_stream)
+    s.upload_state(W0)
+    s.particles_upload(pos0)
+    s.step_timed(args.warmup, True)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    l0 = s.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ph = s.step_timed(args.steps, True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        tdist.barrier()
+    launches = s.launch_count() - l0
+    total_ms = e0.elapsed_time(e1)
+    eul_ms = ph["sweep_x"] + ph["sweep_y"] + ph["sweep_z"] + ph["halo"]
+    part_ms = ph["splines"] + ph["particles"]
+    if dist:
+        t = torch.tensor([eul_ms, part_ms, total_ms], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        eul_ms, part_ms, total_ms = t.tolist()
+
+    # end to end through the plug point evolve(W, dt): pinned host W in, one step, W out
+    nt = s.nt
+    Wh = torch.empty((5, nt, nt, nt), dtype=torch.float64, pin_memory=True)
+    Wn = Wh.numpy()
+    s.download_state(Wn)
+    dt = s.timestep()
+    s.evolve(Wn, dt)   # warm-up of the copy path
+    torch.cuda.synchronize()
+    if dist:
+        tdist.barrier()
+    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    for _ in range(args.steps):
+        s.evolve(Wn, dt)
+    x1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = x0.elapsed_time(x1)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_ms = t.item()
+        tdist.barrier()
+    clocks = sampler.stop()
+    s.close()
+    if rank != 0:
+        return
+
+    cells = n ** 3
+    value = world * cells * args.steps / (eul_ms * 1e-3) / 1e9
+    oc = opcount.load()
+    flops_cell = oc["flops_per_cell_update"]
+    sweep_ms = ph["sweep_x"] + ph["sweep_y"] + ph["sweep_z"]
+    launch_s = sweep_ms * 1e-3 / (3 * args.steps)          # average sweep launch
+    flops_launch = flops_cell * cells / 3                   # one of the three sweeps
+    achieved = flops_launch / launch_s / 1e12
+    bytes_launch = (80 + 120 + 120) / 3 * cells             # compulsory W read + accumulator traffic
+    traffic = None if SWEEP_DRAM_BYTES_PER_CELL is None else SWEEP_DRAM_BYTES_PER_CELL * cells
+    state_bytes = 5 * nt ** 3 * 8
+
+    line = {"metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded solenoidal field (init_DNS recipe), uniform particles",
+            "config": workload(n, npart),
+            "particle_steps_per_s": world * npart * args.steps / (part_ms * 1e-3),
+            "phases_ms_per_step": {k: v / args.steps for k, v in ph.items()},
+            "roofline": {"kernel": "sweep_kernel (x/y/z, one launch each per step)", "bound": "fp64",
+                         "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                         "traffic": traffic, "flops_per_cell_update": flops_cell,
+                         "peak_source": "FP64 FMA probe run by this bench (gkm_probe_fma_peak)",
+                         "hbm": {"achieved_gbs": bytes_launch / launch_s / 1e9, "peak_gbs": HBM_PEAK_GBS,
+                                 "frac": bytes_launch / launch_s / 1e9 / HBM_PEAK_GBS,
+                                 "peak_source": "measured copy bandwidth"}},
+            "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
+            "e2e": {"value": world * cells * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                    "api": "gkm_evolve(h, W, dt): the reference's evolve(W, dev, dt) plug point"},
+            "gpu_launches": launches, "clocks": clocks}
+    if world == 1 and not args.no_cpu_baseline:
+        workers = max(1, min(os.cpu_count() or 1, 8))
+        r = run_reference(workers, 0, 2)
+        line["cpu_baseline"] = {"value": r["gcell"], "unit": "Gcell-updates/s", "cores": workers,
+                                "kind": "reference",
+                                "sample": f"{REF_N}^3 cube per process, same recipe, {REF_PART} particles, 2 steps, "
+                                          f"{workers} concurrent processes ({r['wall_s']:.1f} s wall)",
+                                "particle_steps_per_s": r["psteps"]}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_CELLS)
+    ap.add_argument("--particles", type=int, default=N_PART)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            reference_arm(args, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

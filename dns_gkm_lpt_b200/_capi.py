@@ -23,7 +23,8 @@ EXPORTS = [
     "gkm_upload_state", "gkm_download_state", "gkm_timestep", "gkm_set_dt", "gkm_evolve_eulerian", "gkm_evolve",
     "gkm_step", "gkm_get_clock", "gkm_synchronize", "gkm_particles_upload", "gkm_particles_download",
     "gkm_generate_splines", "gkm_spline_coefs", "gkm_stats_compute", "gkm_flux_faces", "gkm_weno_faces",
-    "gkm_set_stream", "gkm_device_state",
+    "gkm_set_stream", "gkm_device_state", "gkm_evolve_particles", "gkm_step_timed", "gkm_launch_count",
+    "gkm_probe_fma_peak",
 ]
 
 
@@ -82,6 +83,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.gkm_weno_faces.argtypes = [_dp, C.c_int64, C.c_double, _dp, _dp]
     L.gkm_set_stream.argtypes = [_h, C.c_void_p]
     L.gkm_device_state.argtypes = [_h, C.POINTER(_dp)]
+    L.gkm_evolve_particles.argtypes = [_h]
+    L.gkm_step_timed.argtypes = [_h, C.c_int32, C.c_int32, _dp]
+    L.gkm_launch_count.argtypes = [_h, C.POINTER(C.c_int64)]
+    L.gkm_probe_fma_peak.argtypes = [C.c_int32, _dp, _dp]
     for name in EXPORTS:
         if name not in ("gkm_config_default", "gkm_last_error"):
             getattr(L, name).restype = st   # gkm_status, or int for gkm_abi_version / gkm_nt

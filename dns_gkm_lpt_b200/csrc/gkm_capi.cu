@@ -21,7 +21,8 @@ using gkm::FieldConst;
 namespace {
 constexpr int kStatsBlocks = 148 * 4;
 
-enum GraphKind { kGraphEulerian = 0, kGraphFull = 1 };
+enum GraphKind { kGraphEulerian = 0, kGraphFull = 1, kGraphParticles = 2 };
+constexpr int kSplinePasses = 9;   // 3 components x 3 axes
 }  // namespace
 
 struct gkm_handle {
@@ -45,8 +46,10 @@ struct gkm_handle {
     double* P[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // y, x, z, u, v, w
     gkm::StatsPartial* partials = nullptr;
     double* stats_out = nullptr;
-    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    int64_t graph_np[2][2] = {{-1, -1}, {-1, -1}};
+    cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    int64_t graph_np[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
+    int64_t graph_kernels[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    int64_t launches = 0;    // kernels launched (graph replays add the kernels they hold)
     std::string err;
 };
 
@@ -120,7 +123,7 @@ long long coef_count(const gkm_handle* h)
 
 void destroy_graphs(gkm_handle* h)
 {
-    for (int k = 0; k < 2; k++)
+    for (int k = 0; k < 3; k++)
         for (int p = 0; p < 2; p++) {
             if (h->graph[k][p]) cudaGraphExecDestroy(h->graph[k][p]);
             h->graph[k][p] = nullptr;
@@ -144,13 +147,27 @@ cudaError_t enqueue_eulerian(gkm_handle* h)
         cudaError_t e = gkm::launch_sweep(d, a, h->nseg, h->stream);
         if (e != cudaSuccess) return e;
     }
+    h->launches += 4;
     return gkm::launch_halo(h->buf[h->parity ^ 1], h->fc, h->clock, 1, h->stream);
 }
 
 cudaError_t enqueue_splines(gkm_handle* h, const double* W)
 {
+    h->launches += kSplinePasses;
     return gkm::launch_spline_build(W, h->fc, h->grid, device_tables(h), h->coef[0], h->coef[1], h->coef[2],
                                     h->scratch, h->stream);
+}
+
+// splines of the state W and Heun advection with the dt of the last Eulerian step
+cudaError_t enqueue_particles(gkm_handle* h, const double* W)
+{
+    if (h->np <= 0) return cudaSuccess;
+    cudaError_t e = enqueue_splines(h, W);
+    if (e != cudaSuccess) return e;
+    const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+    h->launches += 1;
+    return gkm::launch_particles_heun(c, h->grid, h->clock, h->np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4],
+                                      h->P[5], h->stream);
 }
 
 // the body of Evolve's loop: Eulerian step, splines of the new state, particles
@@ -158,15 +175,14 @@ cudaError_t enqueue_full(gkm_handle* h)
 {
     cudaError_t e = enqueue_eulerian(h);
     if (e != cudaSuccess) return e;
-    const double* Wn = h->buf[h->parity ^ 1];
-    if (h->np > 0) {
-        e = enqueue_splines(h, Wn);
-        if (e != cudaSuccess) return e;
-        const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
-        e = gkm::launch_particles_heun(c, h->grid, h->clock, h->np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4],
-                                       h->P[5], h->stream);
-    }
-    return e;
+    return enqueue_particles(h, h->buf[h->parity ^ 1]);
+}
+
+cudaError_t enqueue_kind(gkm_handle* h, int kind)
+{
+    if (kind == kGraphFull) return enqueue_full(h);
+    if (kind == kGraphParticles) return enqueue_particles(h, h->buf[h->parity]);
+    return enqueue_eulerian(h);
 }
 
 gkm_status run_steps(gkm_handle* h, int32_t nsteps, int kind)
@@ -181,9 +197,12 @@ gkm_status run_steps(gkm_handle* h, int32_t nsteps, int kind)
                 if (h->graph[kind][p]) cudaGraphExecDestroy(h->graph[kind][p]);
                 h->graph[kind][p] = nullptr;
                 cudaGraph_t g = nullptr;
+                const int64_t before = h->launches;
                 CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-                cudaError_t e = kind == kGraphFull ? enqueue_full(h) : enqueue_eulerian(h);
+                cudaError_t e = enqueue_kind(h, kind);
                 cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+                h->graph_kernels[kind][p] = h->launches - before;
+                h->launches = before;   // counted when the graph is replayed
                 if (e != cudaSuccess) return cuda_fail(h, e, "capture step");
                 if (e2 != cudaSuccess) return cuda_fail(h, e2, "cudaStreamEndCapture");
                 e = cudaGraphInstantiate(&h->graph[kind][p], g, 0);
@@ -192,19 +211,21 @@ gkm_status run_steps(gkm_handle* h, int32_t nsteps, int kind)
                 h->graph_np[kind][p] = h->np;
             }
             CK(h, cudaGraphLaunch(h->graph[kind][p], h->stream));
+            h->launches += h->graph_kernels[kind][p];
         } else {
-            cudaError_t e = kind == kGraphFull ? enqueue_full(h) : enqueue_eulerian(h);
+            cudaError_t e = enqueue_kind(h, kind);
             if (e != cudaSuccess) return cuda_fail(h, e, "step launch");
         }
-        h->parity ^= 1;
-        // the particle path leaves the splines of the new state built
-        h->splines_valid = (kind == kGraphFull && h->np > 0);
+        if (kind != kGraphParticles) h->parity ^= 1;
+        // the particle path leaves the splines of the current state built
+        h->splines_valid = (kind != kGraphEulerian && h->np > 0);
     }
     return GKM_OK;
 }
 
 gkm_status reduce_wave(gkm_handle* h)
 {
+    h->launches += 1;
     CK(h, cudaMemsetAsync(&h->clock->wave[h->parity], 0, sizeof(unsigned long long), h->stream));
     CK(h, gkm::launch_wave_reduce(h->buf[h->parity], h->fc, h->clock, h->parity, h->stream));
     return GKM_OK;
@@ -384,6 +405,7 @@ gkm_status gkm_upload_state(gkm_handle* h, const double* const W[5])
     double* dst = h->buf[h->parity];
     for (int q = 0; q < 5; q++)
         CK(h, cudaMemcpyAsync(dst + (size_t)q * h->fc.nt3, W[q], bytes, cudaMemcpyHostToDevice, h->stream));
+    h->launches += 1;
     CK(h, gkm::launch_halo(dst, h->fc, h->clock, 0, h->stream));
     CK(h, cudaMemsetAsync(&h->clock->status, 0, sizeof(int), h->stream));
     gkm_status s = reduce_wave(h);
@@ -438,6 +460,78 @@ gkm_status gkm_set_dt(gkm_handle* h, double dt)
 gkm_status gkm_evolve_eulerian(gkm_handle* h, int32_t nsteps) { return run_steps(h, nsteps, kGraphEulerian); }
 
 gkm_status gkm_step(gkm_handle* h, int32_t nsteps) { return run_steps(h, nsteps, kGraphFull); }
+
+gkm_status gkm_evolve_particles(gkm_handle* h) { return run_steps(h, 1, kGraphParticles); }
+
+gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles, double ms[7])
+{
+    if (!h || !ms || nsteps < 0) return GKM_ERR_ARG;
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    for (int k = 0; k < 7; k++) ms[k] = 0.0;
+    cudaEvent_t ev[7];
+    for (int k = 0; k < 7; k++) CK(h, cudaEventCreate(&ev[k]));
+    gkm_status st = GKM_OK;
+    for (int s = 0; s < nsteps && st == GKM_OK; s++) {
+        gkm::SweepArgs a{};
+        a.W = h->buf[h->parity];
+        a.A = h->buf[h->parity ^ 1];
+        a.fc = h->fc;
+        a.clock = h->clock;
+        a.parity = h->parity;
+        a.dt_fixed_mode = h->dt_fixed_mode;
+        a.dt_fixed = h->dt_fixed;
+        a.seg_len = h->seg_len;
+        cudaError_t e = cudaEventRecord(ev[0], h->stream);
+        for (int d = 0; d < 3 && e == cudaSuccess; d++) {
+            e = gkm::launch_sweep(d, a, h->nseg, h->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[d + 1], h->stream);
+        }
+        if (e == cudaSuccess) e = gkm::launch_halo(h->buf[h->parity ^ 1], h->fc, h->clock, 1, h->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[4], h->stream);
+        h->launches += 4;
+        h->parity ^= 1;
+        const bool parts = with_particles && h->np > 0;
+        if (e == cudaSuccess && parts) e = enqueue_splines(h, h->buf[h->parity]);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[5], h->stream);
+        if (e == cudaSuccess && parts) {
+            const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+            e = gkm::launch_particles_heun(c, h->grid, h->clock, h->np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4],
+                                           h->P[5], h->stream);
+            h->launches += 1;
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ev[6], h->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[6]);
+        if (e != cudaSuccess) {
+            st = cuda_fail(h, e, "gkm_step_timed");
+            break;
+        }
+        float t;
+        for (int k = 0; k < 6; k++) {
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            ms[k] += t;
+        }
+        cudaEventElapsedTime(&t, ev[0], ev[6]);
+        ms[6] += t;
+        h->splines_valid = parts;
+    }
+    for (int k = 0; k < 7; k++) cudaEventDestroy(ev[k]);
+    return st;
+}
+
+gkm_status gkm_launch_count(const gkm_handle* h, int64_t* count)
+{
+    if (!h || !count) return GKM_ERR_ARG;
+    *count = h->launches;
+    return GKM_OK;
+}
+
+gkm_status gkm_probe_fma_peak(int32_t device, double* fp64_tflops, double* fp32_tflops)
+{
+    if (!fp64_tflops || !fp32_tflops) return GKM_ERR_ARG;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = gkm::probe_fma_peak(fp64_tflops, fp32_tflops);
+    return e == cudaSuccess ? GKM_OK : GKM_ERR_CUDA;
+}
 
 gkm_status gkm_evolve(gkm_handle* h, double* const W[5], double dt)
 {
@@ -494,6 +588,7 @@ gkm_status gkm_particles_upload(gkm_handle* h, int64_t np, const double* pos, co
         gkm_status s = ensure_splines(h);
         if (s != GKM_OK) return s;
         const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+        h->launches += 1;
         CK(h, gkm::launch_particles_eval(c, h->grid, np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4], h->P[5],
                                          h->stream));
     }
@@ -541,6 +636,7 @@ gkm_status gkm_stats_compute(gkm_handle* h, gkm_stats* out)
     gkm_status s = ensure_splines(h);
     if (s != GKM_OK) return s;
     const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+    h->launches += 4;
     CK(h, gkm::launch_stats(h->buf[h->parity], h->fc, h->grid, c, h->partials, kStatsBlocks, h->stats_out, h->stream));
     double v[32];
     CK(h, cudaMemcpyAsync(v, h->stats_out, sizeof(v), cudaMemcpyDeviceToHost, h->stream));

@@ -92,4 +92,7 @@ struct StatsPartial {  // per-CTA partial sums of the PrintStats moments
 cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const double* const coefs[3],
                          StatsPartial* partials, int nblocks, double* out16, cudaStream_t s);
 
+// FMA throughput probe (probe.cu)
+cudaError_t probe_fma_peak(double* fp64_tflops, double* fp32_tflops);
+
 }  // namespace gkm

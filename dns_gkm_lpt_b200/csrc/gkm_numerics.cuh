@@ -17,8 +17,17 @@
 // one reciprocal.  The results differ from the reference only by rounding.
 #pragma once
 
-#include <cuda_runtime.h>
 #include <math.h>
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#define GKM_HD __host__ __device__ __forceinline__
+#else
+// host-only compilation (op counting, CPU checks of the device numerics)
+#include <algorithm>
+#include <cmath>
+#define GKM_HD inline
+#endif
 
 namespace gkm {
 
@@ -41,7 +50,7 @@ struct Phys {
 // alpha_k = g_k / (eps + IS_k).  The normalised weights are formed with one
 // division: w_k = g_k prod_{m!=k}(eps+IS_m) / sum_m g_m prod_{m'!=m}(eps+IS_m').
 template <class T>
-__device__ __forceinline__ void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
+GKM_HD void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
 {
     const T c13 = T(1.0 / 3.0), c76 = T(7.0 / 6.0), c116 = T(11.0 / 6.0), c16 = T(1.0 / 6.0), c56 = T(5.0 / 6.0);
     const T c1312 = T(13.0 / 12.0), c14 = T(0.25);
@@ -83,7 +92,7 @@ __device__ __forceinline__ void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, 
 
 // temperature of a conserved state, src/update.cpp:615-620
 template <class T>
-__device__ __forceinline__ T temperature(T r, T m1, T m2, T m3, T E, const Phys<T>& ph)
+GKM_HD T temperature(T r, T m1, T m2, T m3, T E, const Phys<T>& ph)
 {
     T ir = T(1) / r;
     return ph.gm1 * (E * ir - T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) * ir * ir) / ph.Rg;
@@ -91,7 +100,7 @@ __device__ __forceinline__ T temperature(T r, T m1, T m2, T m3, T E, const Phys<
 
 // face energy from reconstructed rho, momentum and temperature, src/update.cpp:673-674
 template <class T>
-__device__ __forceinline__ T face_energy(T r, T m1, T m2, T m3, T Tf, const Phys<T>& ph)
+GKM_HD T face_energy(T r, T m1, T m2, T m3, T Tf, const Phys<T>& ph)
 {
     return r * ph.Rg * Tf / ph.gm1 + T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) / r;
 }
@@ -110,27 +119,27 @@ struct Moments {
 };
 
 template <class T>
-__device__ __forceinline__ T erfc_t(T x);
+GKM_HD T erfc_t(T x);
 template <>
-__device__ __forceinline__ double erfc_t<double>(double x) { return erfc(x); }
+GKM_HD double erfc_t<double>(double x) { return ::erfc(x); }
 template <>
-__device__ __forceinline__ float erfc_t<float>(float x) { return erfcf(x); }
+GKM_HD float erfc_t<float>(float x) { return erfcf(x); }
 template <class T>
-__device__ __forceinline__ T exp_t(T x);
+GKM_HD T exp_t(T x);
 template <>
-__device__ __forceinline__ double exp_t<double>(double x) { return exp(x); }
+GKM_HD double exp_t<double>(double x) { return exp(x); }
 template <>
-__device__ __forceinline__ float exp_t<float>(float x) { return expf(x); }
+GKM_HD float exp_t<float>(float x) { return expf(x); }
 template <class T>
-__device__ __forceinline__ T sqrt_t(T x);
+GKM_HD T sqrt_t(T x);
 template <>
-__device__ __forceinline__ double sqrt_t<double>(double x) { return sqrt(x); }
+GKM_HD double sqrt_t<double>(double x) { return sqrt(x); }
 template <>
-__device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
+GKM_HD float sqrt_t<float>(float x) { return sqrtf(x); }
 
 // half: +1 positive-u half space (erfc(-sqrt(lam) u)/2), -1 negative half
 template <class T>
-__device__ __forceinline__ void half_table(T* H, T U0, T lam, T inv2lam, int half)
+GKM_HD void half_table(T* H, T U0, T lam, T inv2lam, int half)
 {
     const T pi = T(3.14159265358979323846);
     T sl = sqrt_t<T>(lam);
@@ -147,7 +156,7 @@ __device__ __forceinline__ void half_table(T* H, T U0, T lam, T inv2lam, int hal
 }
 
 template <class T, int N>
-__device__ __forceinline__ void full_table(T* F, T U, T inv2lam)
+GKM_HD void full_table(T* F, T U, T inv2lam)
 {
     F[0] = T(1);
     F[1] = U;
@@ -156,7 +165,7 @@ __device__ __forceinline__ void full_table(T* F, T U, T inv2lam)
 }
 
 template <class T>
-__device__ __forceinline__ void build_moments(Moments<T>& M, const T U[3], T lam, int K, int half)
+GKM_HD void build_moments(Moments<T>& M, const T U[3], T lam, int K, int half)
 {
     T inv2lam = T(1) / (T(2) * lam);
     M.Ie2 = T(K) * inv2lam;
@@ -171,7 +180,7 @@ __device__ __forceinline__ void build_moments(Moments<T>& M, const T U[3], T lam
 // <psi (u^k v^l w^m) (a0 + a1 u + a2 v + a3 w + a4 psi4)> with psi = (1,u,v,w,psi4),
 // psi4 = (u^2+v^2+w^2+xi^2)/2; I = normal table (full or half), Y, Z tangential.
 template <int k, int l, int m, class T>
-__device__ __forceinline__ void mcal(T M[5], const T* I, const T* Y, const T* Z, T Ie2, T Ie4, const T a[5])
+GKM_HD void mcal(T M[5], const T* I, const T* Y, const T* Z, T Ie2, T Ie4, const T a[5])
 {
 #define TM(A, B, C) (I[k + (A)] * Y[l + (B)] * Z[m + (C)])
     T t000 = TM(0, 0, 0), t100 = TM(1, 0, 0), t010 = TM(0, 1, 0), t001 = TM(0, 0, 1);
@@ -193,7 +202,7 @@ __device__ __forceinline__ void mcal(T M[5], const T* I, const T* Y, const T* Z,
 }
 
 template <int k, int l, int m, class T>
-__device__ __forceinline__ void mcal0(T M[5], const T* I, const T* Y, const T* Z, T Ie2)
+GKM_HD void mcal0(T M[5], const T* I, const T* Y, const T* Z, T Ie2)
 {
 #define TM(A, B, C) (I[k + (A)] * Y[l + (B)] * Z[m + (C)])
     M[0] = TM(0, 0, 0);
@@ -205,7 +214,7 @@ __device__ __forceinline__ void mcal0(T M[5], const T* I, const T* Y, const T* Z
 }
 
 template <class T>
-__device__ __forceinline__ void axpy5(T* acc, T s, const T* M)
+GKM_HD void axpy5(T* acc, T s, const T* M)
 {
 #pragma unroll
     for (int q = 0; q < 5; q++) acc[q] += s * M[q];
@@ -223,7 +232,7 @@ struct SlopeState {
 };
 
 template <class T>
-__device__ __forceinline__ SlopeState<T> slope_state(const T U[3], T lam, int K)
+GKM_HD SlopeState<T> slope_state(const T U[3], T lam, int K)
 {
     SlopeState<T> s;
     s.U[0] = U[0];
@@ -236,7 +245,7 @@ __device__ __forceinline__ SlopeState<T> slope_state(const T U[3], T lam, int K)
 }
 
 template <class T>
-__device__ __forceinline__ void slope_solve(const T b[5], const SlopeState<T>& s, T a[5])
+GKM_HD void slope_solve(const T b[5], const SlopeState<T>& s, T a[5])
 {
     T r2 = b[1] - s.U[0] * b[0];
     T r3 = b[2] - s.U[1] * b[0];
@@ -250,7 +259,7 @@ __device__ __forceinline__ void slope_solve(const T b[5], const SlopeState<T>& s
 }
 
 template <class T>
-__device__ __forceinline__ void c2p(const T W[5], T gm1, T& den, T U[3], T& P)
+GKM_HD void c2p(const T W[5], T gm1, T& den, T U[3], T& P)
 {
     den = W[0];
     T ir = T(1) / den;
@@ -272,15 +281,15 @@ template <class T>
 struct FaceInput {
     T WL_[5], WR_[5], Wl_[5], Wr_[5];
     T DW_[6][5];
-    __device__ T WL(int q) const { return WL_[q]; }
-    __device__ T WR(int q) const { return WR_[q]; }
-    __device__ T Wl(int q) const { return Wl_[q]; }
-    __device__ T Wr(int q) const { return Wr_[q]; }
-    __device__ T DW(int v, int q) const { return DW_[v][q]; }
+    GKM_HD T WL(int q) const { return WL_[q]; }
+    GKM_HD T WR(int q) const { return WR_[q]; }
+    GKM_HD T Wl(int q) const { return Wl_[q]; }
+    GKM_HD T Wr(int q) const { return Wr_[q]; }
+    GKM_HD T DW(int v, int q) const { return DW_[v][q]; }
 };
 
 template <class T, class Prov>
-__device__ __forceinline__ void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[5])
+GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[5])
 {
     const int K = ph.K;
     T denl, Ul[3], Pl, denr, Ur[3], Pr;

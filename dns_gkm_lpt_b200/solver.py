@@ -121,6 +121,25 @@ class Solver:
     def step(self, nsteps: int = 1) -> None:
         self._check(self.L.gkm_step(self.h, nsteps))
 
+    def evolve_particles(self) -> None:
+        """generateSplines + evolveParticles of the current state (the Lagrangian half of a step)."""
+        self._check(self.L.gkm_evolve_particles(self.h))
+
+    def step_timed(self, nsteps: int, with_particles: bool = True) -> dict:
+        """nsteps with CUDA-event timing of each phase (milliseconds summed over the steps)."""
+        ms = np.zeros(7)
+        self._check(self.L.gkm_step_timed(self.h, nsteps, 1 if with_particles else 0, _ptr(ms)))
+        keys = ("sweep_x", "sweep_y", "sweep_z", "halo", "splines", "particles", "total")
+        return dict(zip(keys, ms.tolist()))
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._check(self.L.gkm_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._check(self.L.gkm_set_stream(self.h, stream_ptr))
+
     def clock(self):
         t, dt, it = C.c_double(), C.c_double(), C.c_int64()
         self._check(self.L.gkm_get_clock(self.h, C.byref(t), C.byref(dt), C.byref(it)))
@@ -157,6 +176,16 @@ class Solver:
         st = _capi.GkmStats()
         self._check(self.L.gkm_stats_compute(self.h, C.byref(st)))
         return st.as_dict()
+
+
+def probe_fma_peak(device: int = 0):
+    """(fp64, fp32) FMA throughput of the device in TFLOP/s."""
+    L = _capi.lib()
+    a, b = C.c_double(), C.c_double()
+    s = L.gkm_probe_fma_peak(device, C.byref(a), C.byref(b))
+    if s != 0:
+        raise GkmError(s, "gkm_probe_fma_peak")
+    return a.value, b.value
 
 
 def flux_faces(inputs: np.ndarray, gam: float, dt: float, dx: float) -> np.ndarray:

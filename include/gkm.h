@@ -139,6 +139,25 @@ gkm_status gkm_evolve(gkm_handle* h, double* const W[5], double dt);
  * src/ParticleTrack.cpp:42-73), dt of the next step.  Asynchronous. */
 gkm_status gkm_step(gkm_handle* h, int32_t nsteps);
 
+/* The Lagrangian half of Evolve's loop body on its own: velocity splines of
+ * the current state, then Heun advection of every particle with the dt of the
+ * last Eulerian step (generateSplines + evolveParticles, src/update.cpp:158-159).
+ * gkm_step(h, n) equals n x { gkm_evolve_eulerian(h, 1); gkm_evolve_particles(h); }. */
+gkm_status gkm_evolve_particles(gkm_handle* h);
+
+/* nsteps full steps (with_particles != 0) or Eulerian steps, with CUDA events
+ * around each phase on the handle's stream; synchronises.  ms[0..6] receive
+ * the summed milliseconds of: x sweep, y sweep, z sweep (incl. the dt
+ * reduction), halo wrap, spline build, particle advection, whole steps. */
+gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles, double ms[7]);
+
+/* Kernels this handle has launched so far (graph replays count their kernels). */
+gkm_status gkm_launch_count(const gkm_handle* h, int64_t* count);
+
+/* Device FMA throughput probe on `device` (independent FMA chains, CUDA-event
+ * timed): FP64 and FP32 in TFLOP/s, an FMA counted as 2 flops. */
+gkm_status gkm_probe_fma_peak(int32_t device, double* fp64_tflops, double* fp32_tflops);
+
 /* t, dt of the last step and completed steps (the globals t, dt, iter of
  * src/update.cpp:6,10).  Synchronises; GKM_ERR_NONFINITE if the state broke. */
 gkm_status gkm_get_clock(gkm_handle* h, double* t, double* dt, int64_t* iter);

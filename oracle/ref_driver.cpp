@@ -265,10 +265,16 @@ void gkmref_stats(double *out16)
  *  eulerian: evolveEulerian + HaloTransfer + timestep   (per step)
  *  particle: velocity splines (generateSplines, 3-field form) + evolveParticles
  *            + the velocity part of getParticleProp at the new positions. */
+void gkmref_particle_props();
+
 void gkmref_time_steps(int nsteps, double *sec_eulerian, double *sec_particles)
 {
 	using clk = std::chrono::steady_clock;
 	double te = 0, tp = 0;
+	/* the reference sets U by getParticleProp before any advection (src/update.cpp:135-136);
+	 * class Particle leaves it uninitialised */
+	if (S.particles && iter == 0)
+		gkmref_particle_props();
 	for (int s = 0; s < nsteps; s++)
 	{
 		UBspline_3d_d *spn[3];

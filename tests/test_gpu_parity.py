@@ -173,3 +173,22 @@ def test_nonfinite_state_is_reported_not_faulted():
         with pytest.raises(GkmError) as e:
             s.timestep()
         assert e.value.status == 4
+
+
+def test_full_size_conservation_and_decay():
+    """256^3: total mass and momentum are conserved to round-off, kinetic energy decays."""
+    P, W0 = case(256, 0.3, 60.0, 1234)
+    sl = slice(3, -3)
+    with Solver(P, cfl=0.5) as s:
+        s.upload_state(W0)
+        e0 = s.print_stats()["TKE"]
+        s.evolve_eulerian(3)
+        W = s.download_state()
+        e1 = s.print_stats()["TKE"]
+    m0 = W0[0, sl, sl, sl].sum(dtype=np.float64)
+    m1 = W[0, sl, sl, sl].sum(dtype=np.float64)
+    assert abs(m1 - m0) <= 1e-12 * m0
+    for q in (1, 2, 3):   # net momentum of the periodic cube stays ~0 (relative to |rho u| scale)
+        scale = np.abs(W0[q, sl, sl, sl]).sum()
+        assert abs(W[q, sl, sl, sl].sum() - W0[q, sl, sl, sl].sum()) <= 1e-12 * scale
+    assert e1 < e0
