@@ -20,7 +20,7 @@ LIBDIR = os.path.join(PKG, "lib")
 OBJDIR = os.path.join(PKG, "lib", "obj")
 LIB = os.path.join(LIBDIR, "libgkm_b200.so")
 
-SOURCES = ["sweep.cu", "lagrangian.cu", "probe.cu", "gkm_capi.cu"]
+SOURCES = ["sweep.cu", "lagrangian.cu", "probe.cu", "noalloc.cu", "gkm_capi.cu"]
 HEADERS = ["gkm_numerics.cuh", "gkm_internal.h"]
 
 NVCC_FLAGS = [

@@ -79,6 +79,8 @@ struct SplineTables {
 
 cudaError_t launch_spline_build(const double* W, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
                                 double* coef_u, double* coef_v, double* coef_w, double* scratch, cudaStream_t s);
+cudaError_t launch_spline_component(const double* W, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
+                                    int component, double* coef, double* scratch, cudaStream_t s);
 cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np,
                                   const double* py, const double* px, const double* pz,
                                   double* Uu, double* Uv, double* Uw, cudaStream_t s);

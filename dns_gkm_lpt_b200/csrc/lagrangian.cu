@@ -384,6 +384,18 @@ cudaError_t launch_spline_build(const double* W, const FieldConst& fc, const Spl
     return cudaSuccess;
 }
 
+// one velocity component (1 = u, 2 = v, 3 = w) with caller-provided scratch and tables
+cudaError_t launch_spline_component(const double* W, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
+                                    int component, double* coef, double* scratch, cudaStream_t s)
+{
+    const long long N = g.npts, M = N + g.pad;
+    cudaError_t e = grid_launch(spline_pass0, N * N, 128, s, W, fc, g, tb, component, coef);
+    if (e != cudaSuccess) return e;
+    e = grid_launch(spline_pass1, M * N, 128, s, (const double*)coef, g, tb, scratch);
+    if (e != cudaSuccess) return e;
+    return grid_launch(spline_pass2, M * M, 128, s, (const double*)scratch, g, tb, coef);
+}
+
 cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np, const double* py,
                                   const double* px, const double* pz, double* Uu, double* Uv, double* Uw,
                                   cudaStream_t s)

@@ -183,6 +183,27 @@ gkm_status gkm_spline_coefs(gkm_handle* h, int32_t c, double* out, int64_t capac
 /* PrintStats field moments (src/update.cpp:688-842) of the current state. */
 gkm_status gkm_stats_compute(gkm_handle* h, gkm_stats* out);
 
+/* Velocity spline of one component built without allocating any device
+ * memory.  No counterpart in the reference (whose einspline build allocates on
+ * the host); it serves callers that cannot call cudaMalloc: programs whose
+ * device memory already belongs to their own pool allocator, and programs
+ * that must not let an allocation synchronise the device.
+ *   W          device pointer to the state, 5 x (n+6)^3 doubles in the
+ *              reference layout with valid ghosts (gkm_device_state gives one)
+ *   component  1 = u, 2 = v, 3 = w (rho u / rho, ...)
+ *   coefs      device pointer to (N+P)^3 doubles (as gkm_spline_coefs)
+ *   stream     cudaStream_t as void*, NULL for the legacy stream
+ * The intermediate results live in one static device array of 32 MiB (plus
+ * 24 KiB of solver tables) that every GPU loading the library holds until
+ * exit; grids needing more (natural_ghost3: about n > 150) return
+ * GKM_ERR_CONFIG with a message on stderr.  The first call on a device looks
+ * up that array's device address, so make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race.  Nothing in the
+ * array needs clearing; every element is written before it is read.
+ * Results equal gkm_generate_splines + gkm_spline_coefs bit for bit. */
+gkm_status gkm_spline_build_noalloc(const double* W, int32_t n, int32_t spline_mode, int32_t component,
+                                    double* coefs, void* stream);
+
 /* ---------------------------------------------------- single-call numerics */
 
 /* flux() of src/GKMflux.cpp:11-229 on nfaces independent faces, host
