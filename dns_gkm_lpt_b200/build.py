@@ -20,8 +20,10 @@ LIBDIR = os.path.join(PKG, "lib")
 OBJDIR = os.path.join(PKG, "lib", "obj")
 LIB = os.path.join(LIBDIR, "libgkm_b200.so")
 
-SOURCES = ["sweep.cu", "lagrangian.cu", "probe.cu", "noalloc.cu", "gkm_capi.cu"]
-HEADERS = ["gkm_numerics.cuh", "gkm_internal.h"]
+SOURCES = ["sweep.cu", "sweep_mixed.cu", "lagrangian.cu", "probe.cu", "noalloc.cu", "gkm_capi.cu"]
+HEADERS = ["gkm_numerics.cuh", "gkm_internal.h", "sweep_impl.cuh"]
+# per-file extra flags: the single-precision sweeps use fast float math
+EXTRA = {"sweep_mixed.cu": ["-use_fast_math"]}
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -56,7 +58,8 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJDIR, src.replace(".cu", ".o"))
         if _stale(o, [s] + deps_common) or ptxas_info:
-            cmd = [nvcc] + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", s, "-o", o]
+            cmd = [nvcc] + NVCC_FLAGS + EXTRA.get(src, []) + (["-Xptxas", "-v"] if ptxas_info else []) + [
+                "-c", s, "-o", o]
             jobs.append(cmd)
 
     def run(cmd):

@@ -131,6 +131,12 @@ void destroy_graphs(gkm_handle* h)
         }
 }
 
+cudaError_t launch_sweep_any(gkm_handle* h, int dir, const gkm::SweepArgs& a)
+{
+    if (h->cfg.precision == GKM_PREC_MIXED) return gkm::launch_sweep_mixed(dir, a, h->nseg, h->stream);
+    return gkm::launch_sweep(dir, a, h->nseg, h->stream);
+}
+
 // enqueue one Eulerian step on h->stream (no host synchronisation)
 cudaError_t enqueue_eulerian(gkm_handle* h)
 {
@@ -144,7 +150,7 @@ cudaError_t enqueue_eulerian(gkm_handle* h)
     a.dt_fixed = h->dt_fixed;
     a.seg_len = h->seg_len;
     for (int d = 0; d < 3; d++) {
-        cudaError_t e = gkm::launch_sweep(d, a, h->nseg, h->stream);
+        cudaError_t e = launch_sweep_any(h, d, a);
         if (e != cudaSuccess) return e;
     }
     h->launches += 4;
@@ -278,7 +284,8 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     if (!(P.gam > 1.0) || !(P.den0 > 0.0) || !(P.p0 > 0.0) || !(P.mu0 >= 0.0) || !(cfg->cfl > 0.0))
         return GKM_ERR_CONFIG;
     if (cfg->visc_law < 0 || cfg->visc_law > 1 || cfg->spline_mode < 0 || cfg->spline_mode > 1) return GKM_ERR_CONFIG;
-    if (cfg->precision != GKM_PREC_FP64 || cfg->max_particles < 0) return GKM_ERR_CONFIG;
+    if (cfg->precision < GKM_PREC_FP64 || cfg->precision > GKM_PREC_MIXED || cfg->max_particles < 0)
+        return GKM_ERR_CONFIG;
     const int K = (int)((5.0 - 3.0 * P.gam) / (P.gam - 1.0));   // src/FlowField.cpp:42
     if (K < 0) return GKM_ERR_CONFIG;
 
@@ -297,6 +304,19 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     fc.mu0 = P.mu0;
     fc.T0 = P.p0 / (287.0 * P.den0);               // src/FlowField.cpp:47
     fc.cfl = cfg->cfl;
+    // working units of the mixed-precision sweeps
+    fc.p0 = P.p0;
+    fc.u_s = std::sqrt(P.p0 / P.den0);
+    fc.inv_rho_s = 1.0 / P.den0;
+    fc.inv_m_s = 1.0 / (P.den0 * fc.u_s);
+    fc.inv_E_s = 1.0 / P.p0;
+    fc.inv_T0 = 1.0 / fc.T0;
+    fc.eps_rho = 1e-10 * fc.inv_rho_s * fc.inv_rho_s;
+    fc.eps_m = 1e-10 * fc.inv_m_s * fc.inv_m_s;
+    fc.eps_T = 1e-10 * fc.inv_T0 * fc.inv_T0;
+    fc.fscale[0] = P.den0 * fc.dx;
+    fc.fscale[1] = fc.fscale[2] = fc.fscale[3] = P.den0 * fc.u_s * fc.dx;
+    fc.fscale[4] = P.p0 * fc.dx;
 
     // segments along the sweep normal: enough CTAs for ~4 waves of 2 CTAs per SM
     const long long tiles = (long long)((fc.n + gkm::kTB - 1) / gkm::kTB) * ((fc.n + gkm::kTA - 1) / gkm::kTA);
@@ -483,7 +503,7 @@ gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles,
         a.seg_len = h->seg_len;
         cudaError_t e = cudaEventRecord(ev[0], h->stream);
         for (int d = 0; d < 3 && e == cudaSuccess; d++) {
-            e = gkm::launch_sweep(d, a, h->nseg, h->stream);
+            e = launch_sweep_any(h, d, a);
             if (e == cudaSuccess) e = cudaEventRecord(ev[d + 1], h->stream);
         }
         if (e == cudaSuccess) e = gkm::launch_halo(h->buf[h->parity ^ 1], h->fc, h->clock, 1, h->stream);

@@ -27,6 +27,12 @@ struct FieldConst {
     int K;
     int visc;       // 0 Sutherland, 1 power law 0.76
     double gam, gm1, dx, inv_dx, mu0, T0, cfl;
+    // mixed-precision working units: rho / rho0, m / (rho0 us), E / p0, T / T0,
+    // lengths in dx, us = sqrt(p0 / rho0); fscale turns a non-dimensional face flux
+    // (time-integrated) back into the dimensional one, per component
+    double p0, u_s, inv_rho_s, inv_m_s, inv_E_s, inv_T0;
+    double eps_rho, eps_m, eps_T;   // the WENO epsilon 1e-10 expressed in those units
+    double fscale[5];
 };
 
 // Sweep geometry: a CTA covers a kTB x kTA window of faces in the plane
@@ -39,7 +45,6 @@ constexpr int kWC = kWA * kWB;      // cells in one slab of the window
 constexpr int kSweepThreads = kTA * kTB;
 constexpr int kRing = 6;            // slabs held: the 6-cell WENO stencil
 constexpr int kSlabComps = 6;       // rho, rho u, rho v, rho w, rho E, T
-constexpr size_t kSweepSmem = sizeof(double) * (size_t)(kRing * kSlabComps * kWC + 10 * kWC);
 
 struct SweepArgs {
     const double* __restrict__ W;   // current state, 5 components of nt^3 (reference layout)
@@ -55,6 +60,8 @@ struct SweepArgs {
 // kernel launchers (sweep.cu); sweep_prepare sets the sweep kernels' shared-memory limit once
 cudaError_t sweep_prepare();
 cudaError_t launch_sweep(int dir, const SweepArgs& a, int nseg, cudaStream_t s);
+// the same sweeps with the reconstruction and the flux in single precision (sweep_mixed.cu)
+cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, int nseg, cudaStream_t s);
 cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, cudaStream_t s);
 cudaError_t launch_wave_reduce(const double* W, const FieldConst& fc, DevClock* clock, int slot, cudaStream_t s);
 cudaError_t launch_flux_faces(const double* in, long long nfaces, double gam, int K, double dt, double dx,

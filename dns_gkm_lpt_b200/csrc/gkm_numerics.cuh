@@ -76,6 +76,18 @@ GKM_HD void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
     d = a1 - T(2) * a2 + a3; e = -T(5) * a1 + T(8) * a2 - T(3) * a3; T I3n = c1312 * d * d + c14 * e * e;
     I3p = fmax(fmax(fmax(I0p, I1p), I2p), I3p);
     I3n = fmax(fmax(fmax(I0n, I1n), I2n), I3n);
+    if constexpr (sizeof(T) == 4) {
+        // single precision: products of three (eps + IS) underflow on flat stencils,
+        // so form the alphas from reciprocals
+        T a0 = T(1) / (eps + I0p), a1 = T(9) / (eps + I1p), a2 = T(9) / (eps + I2p), a3 = T(1) / (eps + I3p);
+        fl = (a0 * P0p + a1 * P1p + a2 * P2p + a3 * P3p) / (a0 + a1 + a2 + a3);
+        a0 = T(1) / (eps + I0n);
+        a1 = T(9) / (eps + I1n);
+        a2 = T(9) / (eps + I2n);
+        a3 = T(1) / (eps + I3n);
+        fr = (a0 * P0n + a1 * P1n + a2 * P2n + a3 * P3n) / (a0 + a1 + a2 + a3);
+        return;
+    }
     {
         T e0 = eps + I0p, e1 = eps + I1p, e2 = eps + I2p, e3 = eps + I3p;
         T p01 = e0 * e1, p23 = e2 * e3;
@@ -269,6 +281,47 @@ GKM_HD void c2p(const T W[5], T gm1, T& den, T U[3], T& P)
     P = (den * gm1) * (W[4] * ir - T(0.5) * (U[0] * U[0] + U[1] * U[1] + U[2] * U[2]));
 }
 
+// ------------------------------------------------- time coefficients ----
+// Integrals over [0, dt] of the BGK relaxation, src/GKMflux.cpp:162-167,197-204.
+// With e = exp(-dt/tau) the coefficients are differences of nearly equal terms
+// when dt/tau is small, so they are always formed in double precision
+// (wide_t), whatever type the flux itself runs in.
+template <class T>
+struct Wide {
+    using type = double;
+};
+template <class T>
+using wide_t = typename Wide<T>::type;
+
+template <class D>
+struct TimeCoefs {
+    D gm1, gm2, gm3, gm4, gm5, p0, p1, p2, p3, p4, p5;
+};
+
+template <class D>
+GKM_HD TimeCoefs<D> time_coefs(D tau, D dt)
+{
+    TimeCoefs<D> c;
+    D ex = exp_t<D>(-dt / tau);
+    D omx = D(1) - ex;
+    D gm0 = dt - tau * omx;
+    D igm0 = D(1) / gm0;
+    c.gm1 = -omx * igm0;
+    c.gm2 = (-dt + D(2) * tau * omx - dt * ex) * igm0;
+    c.gm3 = -c.gm1;
+    c.gm4 = (dt * ex - tau * omx) * igm0;
+    c.gm5 = tau * c.gm3;
+    D Pc = tau * omx;                               // -tau (e - 1)
+    D Qc = -tau * dt * ex + tau * tau * omx;        // -tau dt e - tau^2 (e - 1)
+    c.p0 = dt - Pc;
+    c.p1 = D(0.5) * dt * dt - tau * c.p0;
+    c.p2 = -tau * c.p0 + Qc;
+    c.p3 = Pc;
+    c.p4 = -Qc - tau * Pc;
+    c.p5 = -tau * Pc;
+    return c;
+}
+
 // --------------------------------------------------------- the flux ----
 // The face inputs come from a provider so that the 30 slope values are formed
 // where they are consumed instead of being held in registers.  A provider has
@@ -308,25 +361,10 @@ GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[
 
     // collision time with the pressure-jump correction, src/GKMflux.cpp:156-157
     T ql = denl / laml, qr = denr / lamr;
-    T tau = tau0 + dt * (fabs(ql - qr) / fabs(ql + qr));
-    T ex = exp_t<T>(-dt / tau);
-    T omx = T(1) - ex;
-    // time coefficients, src/GKMflux.cpp:162-167,197-204
-    T gm0 = dt - tau * omx;
-    T igm0 = T(1) / gm0;
-    T gm1 = -omx * igm0;
-    T gm2 = (-dt + T(2) * tau * omx - dt * ex) * igm0;
-    T gm3 = -gm1;
-    T gm4 = (dt * ex - tau * omx) * igm0;
-    T gm5 = tau * gm3;
-    T Pc = tau * omx;                               // -tau (e - 1)
-    T Qc = -tau * dt * ex + tau * tau * omx;        // -tau dt e - tau^2 (e - 1)
-    T p0 = dt - Pc;
-    T p1 = T(0.5) * dt * dt - tau * p0;
-    T p2 = -tau * p0 + Qc;
-    T p3 = Pc;
-    T p4 = -Qc - tau * Pc;
-    T p5 = -tau * Pc;
+    const TimeCoefs<wide_t<T>> tc = time_coefs<wide_t<T>>(
+        wide_t<T>(tau0) + wide_t<T>(dt) * wide_t<T>(fabs(ql - qr) / fabs(ql + qr)), wide_t<T>(dt));
+    const T gm1 = T(tc.gm1), gm2 = T(tc.gm2), gm3 = T(tc.gm3), gm4 = T(tc.gm4), gm5 = T(tc.gm5);
+    const T p0 = T(tc.p0), p1 = T(tc.p1), p2 = T(tc.p2), p3 = T(tc.p3), p4 = T(tc.p4), p5 = T(tc.p5);
 
     T We[5] = {0, 0, 0, 0, 0};      // equilibrium state at the face, src/GKMflux.cpp:73-77
     T by_[5] = {0, 0, 0, 0, 0}, bz_[5] = {0, 0, 0, 0, 0};

@@ -44,6 +44,10 @@ inline Num fmax(Num a, Num b) { g_cnt.cmp++; return Num(std::fmax(a.v, b.v)); }
 
 namespace gkm {
 template <>
+struct Wide<Num> {
+    using type = Num;
+};
+template <>
 inline Num erfc_t<Num>(Num x) { g_cnt.erfc++; return Num(std::erfc(x.v)); }
 template <>
 inline Num exp_t<Num>(Num x) { g_cnt.exp++; return Num(std::exp(x.v)); }

@@ -14,259 +14,13 @@
 // z sweep W' = W - (1/dx) ((A + Fz(k)) - Fz(k-1)) into A; the halo kernel
 // wraps A's ghosts and the caller swaps W and A.  The additions run in the
 // reference's left-to-right order with rounding-explicit intrinsics.
-#include "gkm_internal.h"
-#include "gkm_numerics.cuh"
+#include "sweep_impl.cuh"
 
 namespace gkm {
 namespace {
 
-template <int DIR>
-__device__ __forceinline__ int perm(int q)
-{
-    // face frame: slot 1 holds the normal momentum (y: swap 1<->2, z: swap 1<->3),
-    // src/update.cpp:352-382 and :461-491
-    if (DIR == 1) return q == 1 ? 2 : (q == 2 ? 1 : q);
-    if (DIR == 2) return q == 1 ? 3 : (q == 3 ? 1 : q);
-    return q;
-}
-
-struct Strides {
-    long long sn, sA, sB;
-};
-
-template <int DIR>
-__device__ __forceinline__ Strides strides(int nt)
-{
-    const long long nt2 = (long long)nt * nt;
-    if (DIR == 0) return {nt, nt2, 1};   // normal i; window (j, k)
-    if (DIR == 1) return {nt2, nt, 1};   // normal j; window (i, k)
-    return {1, nt2, nt};                 // normal k; window (j, i)
-}
-
-// Tangential neighbour faces in window coordinates (da, db) and the scale of
-// the first tangential slope.  "N/S" feed the y-slot slope and "F/B" the
-// z-slot slope, as the reference pairs them (src/update.cpp:231-257,303-329,412-438).
-template <int DIR>
-struct Neigh {
-    static constexpr int Na = DIR == 0 ? 1 : (DIR == 1 ? -1 : 0);
-    static constexpr int Nb = DIR == 2 ? 1 : 0;
-    static constexpr int Fa = DIR == 2 ? 1 : 0;
-    static constexpr int Fb = DIR == 2 ? 0 : 1;
-    static constexpr double ys = DIR == 1 ? -0.5 : 0.5;
-};
-
-template <int DIR>
-struct SmemFace {
-    const double* __restrict__ wf;   // slab of the left cell (6 comps x kWC)
-    const double* __restrict__ wf1;  // slab of the right cell
-    const double* __restrict__ rec;  // reconstructions: Wl comps 0..4, Wr comps 5..9
-    int c, cN, cS, cF, cB;
-    double inv_dx;
-    __device__ __forceinline__ double WL(int q) const { return wf[perm<DIR>(q) * kWC + c]; }
-    __device__ __forceinline__ double WR(int q) const { return wf1[perm<DIR>(q) * kWC + c]; }
-    __device__ __forceinline__ double Wl(int q) const { return rec[perm<DIR>(q) * kWC + c]; }
-    __device__ __forceinline__ double Wr(int q) const { return rec[(5 + perm<DIR>(q)) * kWC + c]; }
-    __device__ __forceinline__ double DW(int v, int q) const
-    {
-        const int p = perm<DIR>(q);
-        const double* l = rec + p * kWC;
-        const double* r = rec + (5 + p) * kWC;
-        switch (v) {
-            case 0: return 2.0 * (l[c] - wf[p * kWC + c]) * inv_dx;
-            case 1: return 2.0 * (wf1[p * kWC + c] - r[c]) * inv_dx;
-            case 2: return Neigh<DIR>::ys * (l[cN] - l[cS]) * inv_dx;
-            case 3: return Neigh<DIR>::ys * (r[cN] - r[cS]) * inv_dx;
-            case 4: return 0.5 * (l[cF] - l[cB]) * inv_dx;
-            default: return 0.5 * (r[cF] - r[cB]) * inv_dx;
-        }
-    }
-};
-
-__device__ __forceinline__ double viscosity(const FieldConst& fc, double T)
-{
-    double x = T / fc.T0;
-    if (fc.visc == 1) return fc.mu0 * pow(x, 0.76);
-    return fc.mu0 * (x * sqrt(x)) * (fc.T0 + 110.4) / (T + 110.4);   // Sutherland, src/update.cpp:277
-}
-
-// max(|u| + c) term of one cell with the reference's rounding (src/update.cpp:844-853,1041-1048)
-__device__ __forceinline__ double wave_speed(const double w[5], double gam, double gm1)
-{
-    double d = w[0];
-    double u = __ddiv_rn(w[1], d), v = __ddiv_rn(w[2], d), x = __ddiv_rn(w[3], d);
-    double vs = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(x, x));
-    double p = __dmul_rn(__dmul_rn(d, gm1), __dsub_rn(__ddiv_rn(w[4], d), __dmul_rn(0.5, vs)));
-    return __dadd_rn(__dsqrt_rn(vs), __dsqrt_rn(__ddiv_rn(__dmul_rn(gam, p), d)));
-}
-
-__device__ __forceinline__ double step_dt(const SweepArgs& a)
-{
-    if (a.dt_fixed_mode) return a.dt_fixed;
-    double mw = __longlong_as_double((long long)a.clock->wave[a.parity]);
-    return __ddiv_rn(__dmul_rn(a.fc.cfl, a.fc.dx), mw);   // dt = cfl*dx/maxVAL, src/update.cpp:1053
-}
-
-__device__ __forceinline__ double block_max(double v, double* red)
-{
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    __syncthreads();
-    if ((tid & 31) == 0) red[tid >> 5] = v;
-    __syncthreads();
-    if (tid == 0) {
-        for (int w = 1; w < (int)((blockDim.x * blockDim.y + 31) / 32); w++) v = fmax(v, red[w]);
-    }
-    return v;
-}
-
-template <int DIR>
-__global__ void __launch_bounds__(kSweepThreads, 2) sweep_kernel(SweepArgs a)
-{
-    extern __shared__ double smem[];
-    double* ring = smem;                               // [kRing][kSlabComps][kWC]
-    double* rec = smem + kRing * kSlabComps * kWC;     // [10][kWC]
-    const FieldConst& fc = a.fc;
-    const int n = fc.n, nt = fc.nt;
-    const long long nt3 = fc.nt3;
-    const Strides st = strides<DIR>(nt);
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTB + tx;
-    const int b0 = blockIdx.x * kTB, a0 = blockIdx.y * kTA;
-    const int f_begin = blockIdx.z * a.seg_len;
-    const int f_end = min(f_begin + a.seg_len, n);
-    const double dt = step_dt(a);
-    const Phys<double> ph{fc.gam, fc.gm1, kR, fc.K};
-    const double* __restrict__ W = a.W;
-
-    if (DIR == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0) {
-        a.clock->wave[a.parity ^ 1] = 0ull;   // the z sweep of this step reduces into it
-        a.clock->dt = dt;
-    }
-    if (f_begin >= n) return;
-
-    auto slot = [&](int f) { return ring + ((f + 12) % kRing) * (kSlabComps * kWC); };
-    auto load_slab = [&](int f) {
-        double* s = slot(f);
-        for (int c = tid; c < kWC; c += kSweepThreads) {
-            const int aa = c / kWB, bb = c - aa * kWB;
-            const int A = a0 + aa - 1, B = b0 + bb - 1;
-            if (A > n || B > n) continue;
-            const long long idx = (A + 3) * st.sA + (B + 3) * st.sB + (long long)(f + 3) * st.sn;
-            const double r = W[idx], m1 = W[nt3 + idx], m2 = W[2 * nt3 + idx], m3 = W[3 * nt3 + idx],
-                         E = W[4 * nt3 + idx];
-            s[0 * kWC + c] = r;
-            s[1 * kWC + c] = m1;
-            s[2 * kWC + c] = m2;
-            s[3 * kWC + c] = m3;
-            s[4 * kWC + c] = E;
-            s[5 * kWC + c] = temperature<double>(r, m1, m2, m3, E, ph);
-        }
-    };
-
-    for (int f = f_begin - 3; f < f_begin + 2; f++) load_slab(f);
-
-    const bool active = (a0 + ty < n) && (b0 + tx < n);
-    const int cc = (ty + 1) * kWB + (tx + 1);
-    const long long cell0 = (a0 + ty + 3) * st.sA + (b0 + tx + 3) * st.sB;
-    double Fprev[5] = {0, 0, 0, 0, 0};
-    double wmax = 0.0;
-    bool bad = false;
-
-    for (int f = f_begin - 1; f < f_end; f++) {
-        load_slab(f + 3);
-        __syncthreads();
-        // reconstruct every face of the window once (the reference repeats this 5x per face)
-        {
-            const double* s0 = slot(f - 2);
-            const double* s1 = slot(f - 1);
-            const double* s2 = slot(f);
-            const double* s3 = slot(f + 1);
-            const double* s4 = slot(f + 2);
-            const double* s5 = slot(f + 3);
-            for (int c = tid; c < kWC; c += kSweepThreads) {
-                const int aa = c / kWB, bb = c - aa * kWB;
-                if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
-                double l[5], r[5];
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const int o = q * kWC + c;
-                    weno_scalar<double>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], kWenoEps, l[q], r[q]);
-                }
-                double Tl, Tr;
-                {
-                    const int o = 5 * kWC + c;
-                    weno_scalar<double>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], kWenoEps, Tl, Tr);
-                }
-                l[4] = face_energy<double>(l[0], l[1], l[2], l[3], Tl, ph);
-                r[4] = face_energy<double>(r[0], r[1], r[2], r[3], Tr, ph);
-#pragma unroll
-                for (int q = 0; q < 5; q++) {
-                    rec[q * kWC + c] = l[q];
-                    rec[(5 + q) * kWC + c] = r[q];
-                }
-            }
-        }
-        __syncthreads();
-        if (active) {
-            SmemFace<DIR> pv;
-            pv.wf = slot(f);
-            pv.wf1 = slot(f + 1);
-            pv.rec = rec;
-            pv.c = cc;
-            pv.cN = cc + Neigh<DIR>::Na * kWB + Neigh<DIR>::Nb;
-            pv.cS = cc - Neigh<DIR>::Na * kWB - Neigh<DIR>::Nb;
-            pv.cF = cc + Neigh<DIR>::Fa * kWB + Neigh<DIR>::Fb;
-            pv.cB = cc - Neigh<DIR>::Fa * kWB - Neigh<DIR>::Fb;
-            pv.inv_dx = fc.inv_dx;
-            // collision time of the left cell, mu(T)/p (src/update.cpp:276-278)
-            const double* wl = slot(f);
-            double tau0;
-            {
-                double d = wl[cc], id = 1.0 / d;
-                double u = wl[kWC + cc] * id, v = wl[2 * kWC + cc] * id, w = wl[3 * kWC + cc] * id;
-                double p = (d * fc.gm1) * (wl[4 * kWC + cc] * id - 0.5 * (u * u + v * v + w * w));
-                double T = p / (kR * d);
-                tau0 = viscosity(fc, T) / p;
-            }
-            double Fr[5];
-            gks_flux<double>(pv, tau0, dt, fc.dx, ph, Fr);
-            double F[5];
-#pragma unroll
-            for (int q = 0; q < 5; q++) F[perm<DIR>(q)] = Fr[q];
-            if (f >= f_begin) {
-                const long long ci = cell0 + (long long)(f + 3) * st.sn;
-                if (DIR == 0) {
-#pragma unroll
-                    for (int q = 0; q < 5; q++) a.A[q * nt3 + ci] = __dsub_rn(F[q], Fprev[q]);
-                } else if (DIR == 1) {
-#pragma unroll
-                    for (int q = 0; q < 5; q++) {
-                        double acc = a.A[q * nt3 + ci];
-                        a.A[q * nt3 + ci] = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
-                    }
-                } else {
-                    double wn[5];
-#pragma unroll
-                    for (int q = 0; q < 5; q++) {
-                        double acc = a.A[q * nt3 + ci];
-                        double s = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
-                        wn[q] = __dsub_rn(W[q * nt3 + ci], __dmul_rn(fc.inv_dx, s));
-                        a.A[q * nt3 + ci] = wn[q];
-                    }
-                    double ws = wave_speed(wn, fc.gam, fc.gm1);
-                    if (!isfinite(ws) || !(wn[0] > 0.0)) bad = true;
-                    else wmax = ws > wmax ? ws : wmax;
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 5; q++) Fprev[q] = F[q];
-        }
-    }
-    if (DIR == 2) {
-        double m = block_max(wmax, rec);
-        if (tid == 0 && m > 0.0) atomicMax(&a.clock->wave[a.parity ^ 1], (unsigned long long)__double_as_longlong(m));
-        if (bad) atomicOr(&a.clock->status, 1);
-    }
-}
+using sweep_detail::block_max;
+using sweep_detail::wave_speed;
 
 // Periodic ghost refresh: every ghost cell takes the interior cell at the
 // wrapped index (what HaloTransfer produces on a 1x1x1 periodic topology).
@@ -390,7 +144,7 @@ cudaError_t launch_one(const SweepArgs& a, int nseg, cudaStream_t s)
 {
     dim3 grid((a.fc.n + kTB - 1) / kTB, (a.fc.n + kTA - 1) / kTA, nseg);
     dim3 block(kTB, kTA);
-    sweep_kernel<DIR><<<grid, block, kSweepSmem, s>>>(a);
+    sweep_kernel<DIR, double><<<grid, block, sweep_detail::sweep_smem_bytes<double>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -398,11 +152,12 @@ cudaError_t launch_one(const SweepArgs& a, int nseg, cudaStream_t s)
 
 cudaError_t sweep_prepare()
 {
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmem);
+    const int bytes = (int)sweep_detail::sweep_smem_bytes<double>();
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmem);
+        e = cudaFuncSetAttribute(sweep_kernel<1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmem);
+        e = cudaFuncSetAttribute(sweep_kernel<2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return e;
 }
 

@@ -1,0 +1,312 @@
+// The fused sweep kernel, templated on the face normal DIR and on the type T
+// the reconstruction and the flux run in.  Instantiated for T = double in
+// sweep.cu (the FP64 drop-in) and for T = float in sweep_mixed.cu (the
+// mixed-precision form).  Both read and write the FP64 state and FP64
+// accumulator; the float form converts to non-dimensional single precision
+// when a slab enters shared memory (rho / rho0, m / (rho0 us), E / p0,
+// T / T0 with us = sqrt(p0 / rho0), lengths in dx) and converts each face
+// flux back to dimensional FP64 before the flux difference is accumulated.
+//
+// Reference path: derivsX/Y/Z (src/update.cpp:214-503) -> flux
+// (src/GKMflux.cpp:11-229) -> update (src/update.cpp:505-516), timestep
+// (src/update.cpp:1031-1054).
+#pragma once
+
+#include "gkm_internal.h"
+#include "gkm_numerics.cuh"
+
+namespace gkm {
+namespace sweep_detail {
+
+template <int DIR>
+__device__ __forceinline__ int perm(int q)
+{
+    // face frame: slot 1 holds the normal momentum (y: swap 1<->2, z: swap 1<->3),
+    // src/update.cpp:352-382 and :461-491
+    if (DIR == 1) return q == 1 ? 2 : (q == 2 ? 1 : q);
+    if (DIR == 2) return q == 1 ? 3 : (q == 3 ? 1 : q);
+    return q;
+}
+
+struct Strides {
+    long long sn, sA, sB;
+};
+
+template <int DIR>
+__device__ __forceinline__ Strides strides(int nt)
+{
+    const long long nt2 = (long long)nt * nt;
+    if (DIR == 0) return {nt, nt2, 1};   // normal i; window (j, k)
+    if (DIR == 1) return {nt2, nt, 1};   // normal j; window (i, k)
+    return {1, nt2, nt};                 // normal k; window (j, i)
+}
+
+// Tangential neighbour faces in window coordinates (da, db) and the scale of
+// the first tangential slope.  "N/S" feed the y-slot slope and "F/B" the
+// z-slot slope, as the reference pairs them (src/update.cpp:231-257,303-329,412-438).
+template <int DIR>
+struct Neigh {
+    static constexpr int Na = DIR == 0 ? 1 : (DIR == 1 ? -1 : 0);
+    static constexpr int Nb = DIR == 2 ? 1 : 0;
+    static constexpr int Fa = DIR == 2 ? 1 : 0;
+    static constexpr int Fb = DIR == 2 ? 0 : 1;
+    static constexpr double ys = DIR == 1 ? -0.5 : 0.5;
+};
+
+template <int DIR, class T>
+struct SmemFace {
+    const T* __restrict__ wf;   // slab of the left cell (6 comps x kWC)
+    const T* __restrict__ wf1;  // slab of the right cell
+    const T* __restrict__ rec;  // reconstructions: Wl comps 0..4, Wr comps 5..9
+    int c, cN, cS, cF, cB;
+    T inv_dx;
+    __device__ __forceinline__ T WL(int q) const { return wf[perm<DIR>(q) * kWC + c]; }
+    __device__ __forceinline__ T WR(int q) const { return wf1[perm<DIR>(q) * kWC + c]; }
+    __device__ __forceinline__ T Wl(int q) const { return rec[perm<DIR>(q) * kWC + c]; }
+    __device__ __forceinline__ T Wr(int q) const { return rec[(5 + perm<DIR>(q)) * kWC + c]; }
+    __device__ __forceinline__ T DW(int v, int q) const
+    {
+        const int p = perm<DIR>(q);
+        const T* l = rec + p * kWC;
+        const T* r = rec + (5 + p) * kWC;
+        const T ys = T(Neigh<DIR>::ys);
+        switch (v) {
+            case 0: return T(2) * (l[c] - wf[p * kWC + c]) * inv_dx;
+            case 1: return T(2) * (wf1[p * kWC + c] - r[c]) * inv_dx;
+            case 2: return ys * (l[cN] - l[cS]) * inv_dx;
+            case 3: return ys * (r[cN] - r[cS]) * inv_dx;
+            case 4: return T(0.5) * (l[cF] - l[cB]) * inv_dx;
+            default: return T(0.5) * (r[cF] - r[cB]) * inv_dx;
+        }
+    }
+};
+
+__device__ __forceinline__ double viscosity(const FieldConst& fc, double T)
+{
+    double x = T / fc.T0;
+    if (fc.visc == 1) return fc.mu0 * pow(x, 0.76);
+    return fc.mu0 * (x * sqrt(x)) * (fc.T0 + 110.4) / (T + 110.4);   // Sutherland, src/update.cpp:277
+}
+
+// max(|u| + c) term of one cell with the reference's rounding (src/update.cpp:844-853,1041-1048)
+__device__ __forceinline__ double wave_speed(const double w[5], double gam, double gm1)
+{
+    double d = w[0];
+    double u = __ddiv_rn(w[1], d), v = __ddiv_rn(w[2], d), x = __ddiv_rn(w[3], d);
+    double vs = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(x, x));
+    double p = __dmul_rn(__dmul_rn(d, gm1), __dsub_rn(__ddiv_rn(w[4], d), __dmul_rn(0.5, vs)));
+    return __dadd_rn(__dsqrt_rn(vs), __dsqrt_rn(__ddiv_rn(__dmul_rn(gam, p), d)));
+}
+
+__device__ __forceinline__ double step_dt(const SweepArgs& a)
+{
+    if (a.dt_fixed_mode) return a.dt_fixed;
+    double mw = __longlong_as_double((long long)a.clock->wave[a.parity]);
+    return __ddiv_rn(__dmul_rn(a.fc.cfl, a.fc.dx), mw);   // dt = cfl*dx/maxVAL, src/update.cpp:1053
+}
+
+__device__ __forceinline__ double block_max(double v, double* red)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    __syncthreads();
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < (int)((blockDim.x * blockDim.y + 31) / 32); w++) v = fmax(v, red[w]);
+    }
+    return v;
+}
+
+template <class T>
+constexpr size_t sweep_smem_bytes()
+{
+    return sizeof(T) * (size_t)(kRing * kSlabComps * kWC + 10 * kWC);
+}
+
+template <class T>
+struct SweepOccupancy {
+    static constexpr int ctas = sizeof(T) == 8 ? 2 : 3;   // CTAs of 128 threads per SM the registers allow
+};
+
+}  // namespace sweep_detail
+
+template <int DIR, class T>
+__global__ void __launch_bounds__(kSweepThreads, sweep_detail::SweepOccupancy<T>::ctas) sweep_kernel(SweepArgs a)
+{
+    using namespace sweep_detail;
+    constexpr bool kMixed = sizeof(T) == 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* ring = reinterpret_cast<T*>(smem_raw);          // [kRing][kSlabComps][kWC]
+    T* rec = ring + kRing * kSlabComps * kWC;          // [10][kWC]
+    const FieldConst& fc = a.fc;
+    const int n = fc.n, nt = fc.nt;
+    const long long nt3 = fc.nt3;
+    const Strides st = strides<DIR>(nt);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTB + tx;
+    const int b0 = blockIdx.x * kTB, a0 = blockIdx.y * kTA;
+    const int f_begin = blockIdx.z * a.seg_len;
+    const int f_end = min(f_begin + a.seg_len, n);
+    const double dt = step_dt(a);
+    // working units: dimensional for double, non-dimensional (dx = 1) for float
+    const T dtw = kMixed ? T(dt * fc.u_s * fc.inv_dx) : T(dt);
+    const T dxw = kMixed ? T(1) : T(fc.dx);
+    const T inv_dxw = kMixed ? T(1) : T(fc.inv_dx);
+    const Phys<T> ph{T(fc.gam), T(fc.gm1), kMixed ? T(1) : T(kR), fc.K};
+    const T eps_r = kMixed ? T(fc.eps_rho) : T(kWenoEps);
+    const T eps_m = kMixed ? T(fc.eps_m) : T(kWenoEps);
+    const T eps_T = kMixed ? T(fc.eps_T) : T(kWenoEps);
+    const double* __restrict__ W = a.W;
+
+    if (DIR == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0) {
+        a.clock->wave[a.parity ^ 1] = 0ull;   // the z sweep of this step reduces into it
+        a.clock->dt = dt;
+    }
+    if (f_begin >= n) return;
+
+    auto slot = [&](int f) { return ring + ((f + 12) % kRing) * (kSlabComps * kWC); };
+    auto load_slab = [&](int f) {
+        T* s = slot(f);
+        for (int c = tid; c < kWC; c += kSweepThreads) {
+            const int aa = c / kWB, bb = c - aa * kWB;
+            const int A = a0 + aa - 1, B = b0 + bb - 1;
+            if (A > n || B > n) continue;
+            const long long idx = (A + 3) * st.sA + (B + 3) * st.sB + (long long)(f + 3) * st.sn;
+            const double r = W[idx], m1 = W[nt3 + idx], m2 = W[2 * nt3 + idx], m3 = W[3 * nt3 + idx],
+                         E = W[4 * nt3 + idx];
+            if constexpr (kMixed) {
+                const double Tk = temperature<double>(r, m1, m2, m3, E, Phys<double>{fc.gam, fc.gm1, kR, fc.K});
+                s[0 * kWC + c] = T(r * fc.inv_rho_s);
+                s[1 * kWC + c] = T(m1 * fc.inv_m_s);
+                s[2 * kWC + c] = T(m2 * fc.inv_m_s);
+                s[3 * kWC + c] = T(m3 * fc.inv_m_s);
+                s[4 * kWC + c] = T(E * fc.inv_E_s);
+                s[5 * kWC + c] = T(Tk * fc.inv_T0);
+            } else {
+                s[0 * kWC + c] = r;
+                s[1 * kWC + c] = m1;
+                s[2 * kWC + c] = m2;
+                s[3 * kWC + c] = m3;
+                s[4 * kWC + c] = E;
+                s[5 * kWC + c] = temperature<double>(r, m1, m2, m3, E, ph);
+            }
+        }
+    };
+
+    for (int f = f_begin - 3; f < f_begin + 2; f++) load_slab(f);
+
+    const bool active = (a0 + ty < n) && (b0 + tx < n);
+    const int cc = (ty + 1) * kWB + (tx + 1);
+    const long long cell0 = (a0 + ty + 3) * st.sA + (b0 + tx + 3) * st.sB;
+    double Fprev[5] = {0, 0, 0, 0, 0};
+    double wmax = 0.0;
+    bool bad = false;
+
+    for (int f = f_begin - 1; f < f_end; f++) {
+        load_slab(f + 3);
+        __syncthreads();
+        // reconstruct every face of the window once (the reference repeats this 5x per face)
+        {
+            const T* s0 = slot(f - 2);
+            const T* s1 = slot(f - 1);
+            const T* s2 = slot(f);
+            const T* s3 = slot(f + 1);
+            const T* s4 = slot(f + 2);
+            const T* s5 = slot(f + 3);
+            for (int c = tid; c < kWC; c += kSweepThreads) {
+                const int aa = c / kWB, bb = c - aa * kWB;
+                if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
+                T l[5], r[5];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int o = q * kWC + c;
+                    weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], q == 0 ? eps_r : eps_m, l[q], r[q]);
+                }
+                T Tl, Tr;
+                {
+                    const int o = 5 * kWC + c;
+                    weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], eps_T, Tl, Tr);
+                }
+                l[4] = face_energy<T>(l[0], l[1], l[2], l[3], Tl, ph);
+                r[4] = face_energy<T>(r[0], r[1], r[2], r[3], Tr, ph);
+#pragma unroll
+                for (int q = 0; q < 5; q++) {
+                    rec[q * kWC + c] = l[q];
+                    rec[(5 + q) * kWC + c] = r[q];
+                }
+            }
+        }
+        __syncthreads();
+        if (active) {
+            SmemFace<DIR, T> pv;
+            pv.wf = slot(f);
+            pv.wf1 = slot(f + 1);
+            pv.rec = rec;
+            pv.c = cc;
+            pv.cN = cc + Neigh<DIR>::Na * kWB + Neigh<DIR>::Nb;
+            pv.cS = cc - Neigh<DIR>::Na * kWB - Neigh<DIR>::Nb;
+            pv.cF = cc + Neigh<DIR>::Fa * kWB + Neigh<DIR>::Fb;
+            pv.cB = cc - Neigh<DIR>::Fa * kWB - Neigh<DIR>::Fb;
+            pv.inv_dx = inv_dxw;
+            // collision time of the left cell, mu(T)/p (src/update.cpp:276-278)
+            const T* wl = slot(f);
+            T tau0;
+            if constexpr (kMixed) {
+                // p' = p / p0 and T' = T / T0 in the working units; tau' = tau us / dx
+                const float d = wl[cc], id = 1.0f / d;
+                const float u = wl[kWC + cc] * id, v = wl[2 * kWC + cc] * id, w = wl[3 * kWC + cc] * id;
+                const float p = (d * float(fc.gm1)) * (wl[4 * kWC + cc] * id - 0.5f * (u * u + v * v + w * w));
+                const double Tk = (double)(p * id) * fc.T0;
+                tau0 = T(viscosity(fc, Tk) / ((double)p * fc.p0) * fc.u_s * fc.inv_dx);
+            } else {
+                double d = wl[cc], id = 1.0 / d;
+                double u = wl[kWC + cc] * id, v = wl[2 * kWC + cc] * id, w = wl[3 * kWC + cc] * id;
+                double p = (d * fc.gm1) * (wl[4 * kWC + cc] * id - 0.5 * (u * u + v * v + w * w));
+                double Tk = p / (kR * d);
+                tau0 = viscosity(fc, Tk) / p;
+            }
+            T Fr[5];
+            gks_flux<T>(pv, tau0, dtw, dxw, ph, Fr);
+            double F[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                if constexpr (kMixed) F[perm<DIR>(q)] = (double)Fr[q] * fc.fscale[perm<DIR>(q)];
+                else F[perm<DIR>(q)] = Fr[q];
+            }
+            if (f >= f_begin) {
+                const long long ci = cell0 + (long long)(f + 3) * st.sn;
+                if (DIR == 0) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) a.A[q * nt3 + ci] = __dsub_rn(F[q], Fprev[q]);
+                } else if (DIR == 1) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) {
+                        double acc = a.A[q * nt3 + ci];
+                        a.A[q * nt3 + ci] = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
+                    }
+                } else {
+                    double wn[5];
+#pragma unroll
+                    for (int q = 0; q < 5; q++) {
+                        double acc = a.A[q * nt3 + ci];
+                        double s = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
+                        wn[q] = __dsub_rn(W[q * nt3 + ci], __dmul_rn(fc.inv_dx, s));
+                        a.A[q * nt3 + ci] = wn[q];
+                    }
+                    double ws = wave_speed(wn, fc.gam, fc.gm1);
+                    if (!isfinite(ws) || !(wn[0] > 0.0)) bad = true;
+                    else wmax = ws > wmax ? ws : wmax;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 5; q++) Fprev[q] = F[q];
+        }
+    }
+    if (DIR == 2) {
+        double m = block_max(wmax, reinterpret_cast<double*>(rec));
+        if (tid == 0 && m > 0.0) atomicMax(&a.clock->wave[a.parity ^ 1], (unsigned long long)__double_as_longlong(m));
+        if (bad) atomicOr(&a.clock->status, 1);
+    }
+}
+
+}  // namespace gkm

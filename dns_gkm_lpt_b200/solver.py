@@ -49,7 +49,7 @@ def _w5(W: np.ndarray):
 
 class Solver:
     def __init__(self, params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
-                 max_particles: int = 0, device: int = 0, use_graphs: bool = True):
+                 max_particles: int = 0, device: int = 0, use_graphs: bool = True, precision: int = 0):
         self.L = _capi.lib()
         cfg = _capi.GkmConfig()
         self.L.gkm_config_default(C.byref(cfg))
@@ -61,6 +61,7 @@ class Solver:
         cfg.device = device
         cfg.max_particles = max_particles
         cfg.use_graphs = 1 if use_graphs else 0
+        cfg.precision = precision   # 0 FP64, 1 mixed (FP32 reconstruction + flux, FP64 state)
         h = C.c_void_p()
         s = self.L.gkm_create(C.byref(cfg), C.byref(h))
         if s != 0:

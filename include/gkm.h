@@ -51,7 +51,9 @@ typedef enum gkm_spline_mode {
 } gkm_spline_mode;
 
 typedef enum gkm_precision {
-    GKM_PREC_FP64 = 0 /* FP64 everywhere (the reference's ptype = double) */
+    GKM_PREC_FP64 = 0, /* FP64 everywhere (the reference's ptype = double) */
+    GKM_PREC_MIXED = 1 /* WENO + gas-kinetic flux in FP32 on non-dimensional values; BGK time
+                          coefficients, flux differences, the update, dt and all reductions in FP64 */
 } gkm_precision;
 
 /* Contents of InitialConditions/params, read by GetParams (src/FlowField.cpp:9-58). */

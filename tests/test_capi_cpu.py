@@ -59,7 +59,7 @@ def test_create_rejects_bad_enums_and_null():
     L.gkm_config_default(C.byref(cfg))
     cfg.params.n, cfg.params.gam, cfg.params.den0, cfg.params.p0, cfg.params.mu0 = 16, 1.4, 1.0, 86100.0, 1.0
     h = C.c_void_p()
-    for f, v in (("spline_mode", 7), ("visc_law", -1), ("precision", 3)):
+    for f, v in (("spline_mode", 7), ("visc_law", -1), ("precision", 3), ("precision", -1)):
         c2 = _capi.GkmConfig.from_buffer_copy(cfg)
         setattr(c2, f, v)
         assert L.gkm_create(C.byref(c2), C.byref(h)) == _capi.GKM_ERR_CONFIG
