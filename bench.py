@@ -45,6 +45,10 @@ HBM_PEAK_GBS = 6550.7        # measured copy bandwidth of this pool's B200s
 SWEEP_DRAM_BYTES_PER_CELL = 102.8   # profiles/sweep_kernel_fp64_128cube_full.md, mean of x/y/z
 
 
+def cells_of(n: int) -> int:
+    return n ** 3
+
+
 def workload(n=N_CELLS, npart=N_PART):
     return {"workload": f"{n}^3 periodic cube, FP64 drop-in, Mt {MT}, Re_lambda {RE:g}, {npart} particles, "
                         f"cfl {CFL}, natural_ghost3 splines",
@@ -168,6 +172,7 @@ def ours(args, rank: int, world: int, local_rank: int):
     s.set_stream(stream.cuda_stream)
     s.upload_state(W0)
     s.particles_upload(pos0)
+    sweep_cfg = s.autotune(2)
     s.step_timed(args.warmup, True)
     torch.cuda.synchronize()
 
@@ -193,8 +198,35 @@ def ours(args, rank: int, world: int, local_rank: int):
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         eul_ms, part_ms, total_ms = t.tolist()
 
-    # end to end through the plug point evolve(W, dt): pinned host W in, one step, W out
+    # the mixed-precision form on the same input and step count; error against this FP64 run
     nt = s.nt
+    forms = {}
+    if not args.no_forms:
+        W64 = s.download_state()
+        tke64 = s.print_stats()["TKE"]
+        m = Solver(P, cfl=CFL, max_particles=npart, device=local_rank, precision=1)
+        m.set_stream(stream.cuda_stream)
+        m.upload_state(W0)
+        m.particles_upload(pos0)
+        m_cfg = m.autotune(2)
+        m.step_timed(args.warmup, True)
+        mph = m.step_timed(args.steps, True)
+        Wm = m.download_state()
+        tkem = m.print_stats()["TKE"]
+        m.close()
+        sl = slice(3, -3)
+        err = [float(np.linalg.norm(Wm[q, sl, sl, sl] - W64[q, sl, sl, sl]) / np.linalg.norm(W64[q, sl, sl, sl]))
+               for q in range(5)]
+        m_eul = mph["sweep_x"] + mph["sweep_y"] + mph["sweep_z"] + mph["halo"]
+        forms["mixed"] = {"value": world * cells_of(n) * args.steps / (m_eul * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+                          "particle_steps_per_s": world * npart * args.steps / ((mph["splines"] + mph["particles"]) * 1e-3),
+                          "ms_per_step": mph["total"] / args.steps,
+                          "rel_l2_vs_fp64": dict(zip(("rho", "rho_u", "rho_v", "rho_w", "rho_E"), err)),
+                          "tke_rel_err_vs_fp64": abs(tkem - tke64) / tke64,
+                          "steps_compared": args.warmup + args.steps, "sweep_shapes": m_cfg}
+        del W64, Wm
+
+    # end to end through the plug point evolve(W, dt): pinned host W in, one step, W out
     Wh = torch.empty((5, nt, nt, nt), dtype=torch.float64, pin_memory=True)
     Wn = Wh.numpy()
     s.download_state(Wn)
@@ -250,7 +282,7 @@ def ours(args, rank: int, world: int, local_rank: int):
             "e2e": {"value": world * cells * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
                     "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                     "api": "gkm_evolve(h, W, dt): the reference's evolve(W, dev, dt) plug point"},
-            "gpu_launches": launches, "clocks": clocks}
+            "gpu_launches": launches, "clocks": clocks, "sweep_shapes": sweep_cfg, "forms": forms}
     if world == 1 and not args.no_cpu_baseline:
         workers = max(1, min(os.cpu_count() or 1, 8))
         r = run_reference(workers, 0, 2)
@@ -271,6 +303,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_CELLS)
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed-precision form")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -24,7 +24,7 @@ EXPORTS = [
     "gkm_step", "gkm_get_clock", "gkm_synchronize", "gkm_particles_upload", "gkm_particles_download",
     "gkm_generate_splines", "gkm_spline_coefs", "gkm_stats_compute", "gkm_flux_faces", "gkm_weno_faces",
     "gkm_set_stream", "gkm_device_state", "gkm_evolve_particles", "gkm_step_timed", "gkm_launch_count",
-    "gkm_probe_fma_peak", "gkm_spline_build_noalloc",
+    "gkm_probe_fma_peak", "gkm_spline_build_noalloc", "gkm_autotune", "gkm_sweep_config",
 ]
 
 
@@ -87,6 +87,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.gkm_step_timed.argtypes = [_h, C.c_int32, C.c_int32, _dp]
     L.gkm_launch_count.argtypes = [_h, C.POINTER(C.c_int64)]
     L.gkm_probe_fma_peak.argtypes = [C.c_int32, _dp, _dp]
+    L.gkm_autotune.argtypes = [_h, C.c_int32]
+    L.gkm_sweep_config.argtypes = [_h, C.POINTER(C.c_int32)]
     L.gkm_spline_build_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
     for name in EXPORTS:
         if name not in ("gkm_config_default", "gkm_last_error"):

@@ -25,10 +25,16 @@ enum GraphKind { kGraphEulerian = 0, kGraphFull = 1, kGraphParticles = 2 };
 constexpr int kSplinePasses = 9;   // 3 components x 3 axes
 }  // namespace
 
+struct SweepChoice {
+    int variant = 0;   // window variant (gkm::sweep_shape)
+    int nseg = 1;      // CTAs along the sweep normal
+    int seg_len = 1;   // faces per CTA along the normal
+};
+
 struct gkm_handle {
     gkm_config cfg{};
     FieldConst fc{};
-    int nseg = 1, seg_len = 1;
+    SweepChoice sweep[3];
     cudaStream_t own_stream = nullptr, stream = nullptr;
     double* buf[2] = {nullptr, nullptr};
     int parity = 0;
@@ -131,10 +137,28 @@ void destroy_graphs(gkm_handle* h)
         }
 }
 
-cudaError_t launch_sweep_any(gkm_handle* h, int dir, const gkm::SweepArgs& a)
+cudaError_t launch_sweep_any(gkm_handle* h, int dir, gkm::SweepArgs a)
 {
-    if (h->cfg.precision == GKM_PREC_MIXED) return gkm::launch_sweep_mixed(dir, a, h->nseg, h->stream);
-    return gkm::launch_sweep(dir, a, h->nseg, h->stream);
+    const SweepChoice& c = h->sweep[dir];
+    a.seg_len = c.seg_len;
+    if (h->cfg.precision == GKM_PREC_MIXED) return gkm::launch_sweep_mixed(dir, c.variant, a, c.nseg, h->stream);
+    return gkm::launch_sweep(dir, c.variant, a, c.nseg, h->stream);
+}
+
+// segments along the sweep normal: enough CTAs for ~4 waves of the CTAs an SM holds
+SweepChoice default_choice(const FieldConst& fc, bool mixed, int variant)
+{
+    const gkm::SweepShape sh = gkm::sweep_shape(mixed, variant);
+    const long long tiles = (long long)((fc.n + sh.TB - 1) / sh.TB) * ((fc.n + sh.TA - 1) / sh.TA);
+    long long nseg = (148LL * sh.ctas * 4 + tiles - 1) / tiles;
+    long long maxseg = fc.n / 16 > 1 ? fc.n / 16 : 1;
+    if (nseg > maxseg) nseg = maxseg;
+    if (nseg < 1) nseg = 1;
+    SweepChoice c;
+    c.variant = variant;
+    c.seg_len = (int)((fc.n + nseg - 1) / nseg);
+    c.nseg = (fc.n + c.seg_len - 1) / c.seg_len;
+    return c;
 }
 
 // enqueue one Eulerian step on h->stream (no host synchronisation)
@@ -148,7 +172,6 @@ cudaError_t enqueue_eulerian(gkm_handle* h)
     a.parity = h->parity;
     a.dt_fixed_mode = h->dt_fixed_mode;
     a.dt_fixed = h->dt_fixed;
-    a.seg_len = h->seg_len;
     for (int d = 0; d < 3; d++) {
         cudaError_t e = launch_sweep_any(h, d, a);
         if (e != cudaSuccess) return e;
@@ -318,14 +341,7 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     fc.fscale[1] = fc.fscale[2] = fc.fscale[3] = P.den0 * fc.u_s * fc.dx;
     fc.fscale[4] = P.p0 * fc.dx;
 
-    // segments along the sweep normal: enough CTAs for ~4 waves of 2 CTAs per SM
-    const long long tiles = (long long)((fc.n + gkm::kTB - 1) / gkm::kTB) * ((fc.n + gkm::kTA - 1) / gkm::kTA);
-    long long nseg = (148LL * 2 * 4 + tiles - 1) / tiles;
-    long long maxseg = fc.n / 16 > 1 ? fc.n / 16 : 1;
-    if (nseg > maxseg) nseg = maxseg;
-    if (nseg < 1) nseg = 1;
-    h->seg_len = (int)((fc.n + nseg - 1) / nseg);
-    h->nseg = (int)((fc.n + h->seg_len - 1) / h->seg_len);
+    for (int d = 0; d < 3; d++) h->sweep[d] = default_choice(fc, cfg->precision == GKM_PREC_MIXED, 0);
 
     auto bail = [&](cudaError_t e, const char* where) {
         gkm_status s = cuda_fail(h, e, where);
@@ -393,6 +409,7 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     e = cudaMalloc(&h->stats_out, sizeof(double) * 32);
     if (e != cudaSuccess) return bail(e, "cudaMalloc(stats)");
     e = gkm::sweep_prepare();
+    if (e == cudaSuccess) e = gkm::sweep_mixed_prepare();
     if (e != cudaSuccess) return bail(e, "sweep_prepare");
     *out = h;
     return GKM_OK;
@@ -500,7 +517,6 @@ gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles,
         a.parity = h->parity;
         a.dt_fixed_mode = h->dt_fixed_mode;
         a.dt_fixed = h->dt_fixed;
-        a.seg_len = h->seg_len;
         cudaError_t e = cudaEventRecord(ev[0], h->stream);
         for (int d = 0; d < 3 && e == cudaSuccess; d++) {
             e = launch_sweep_any(h, d, a);
@@ -536,6 +552,84 @@ gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles,
     }
     for (int k = 0; k < 7; k++) cudaEventDestroy(ev[k]);
     return st;
+}
+
+gkm_status gkm_autotune(gkm_handle* h, int32_t reps)
+{
+    if (!h || reps < 1) return GKM_ERR_ARG;
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    const bool mixed = h->cfg.precision == GKM_PREC_MIXED;
+    const int nvar = mixed ? gkm::kSweepVariants32 : gkm::kSweepVariants64;
+    // the sweeps leave W untouched (they write the accumulator A only); the clock
+    // they also touch is saved here and put back afterwards
+    DevClock saved;
+    CK(h, cudaMemcpyAsync(&saved, h->clock, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    cudaEvent_t e0, e1;
+    CK(h, cudaEventCreate(&e0));
+    CK(h, cudaEventCreate(&e1));
+    gkm::SweepArgs a{};
+    a.W = h->buf[h->parity];
+    a.A = h->buf[h->parity ^ 1];
+    a.fc = h->fc;
+    a.clock = h->clock;
+    a.parity = h->parity;
+    a.dt_fixed_mode = h->dt_fixed_mode;
+    a.dt_fixed = h->dt_fixed;
+    const int nsegs[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16, 24, 32};
+    gkm_status st = GKM_OK;
+    for (int d = 0; d < 3 && st == GKM_OK; d++) {
+        SweepChoice best = h->sweep[d];
+        float best_ms = 1e30f;
+        for (int v = 0; v < nvar && st == GKM_OK; v++) {
+            int last_len = -1;
+            for (int ns : nsegs) {
+                SweepChoice c;
+                c.variant = v;
+                c.seg_len = (h->fc.n + ns - 1) / ns;
+                if (c.seg_len < 8 || c.seg_len == last_len) continue;
+                last_len = c.seg_len;
+                c.nseg = (h->fc.n + c.seg_len - 1) / c.seg_len;
+                h->sweep[d] = c;
+                cudaError_t e = launch_sweep_any(h, d, a);   // warm-up
+                if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
+                for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch_sweep_any(h, d, a);
+                if (e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                if (e != cudaSuccess) {
+                    st = cuda_fail(h, e, "gkm_autotune");
+                    break;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = c;
+                }
+            }
+        }
+        h->sweep[d] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaMemcpyAsync(h->clock, &saved, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+    destroy_graphs(h);
+    return st;
+}
+
+gkm_status gkm_sweep_config(const gkm_handle* h, int32_t out[12])
+{
+    if (!h || !out) return GKM_ERR_ARG;
+    const bool mixed = h->cfg.precision == GKM_PREC_MIXED;
+    for (int d = 0; d < 3; d++) {
+        const gkm::SweepShape sh = gkm::sweep_shape(mixed, h->sweep[d].variant);
+        out[4 * d + 0] = h->sweep[d].variant;
+        out[4 * d + 1] = sh.TB;
+        out[4 * d + 2] = sh.TA;
+        out[4 * d + 3] = h->sweep[d].seg_len;
+    }
+    return GKM_OK;
 }
 
 gkm_status gkm_launch_count(const gkm_handle* h, int64_t* count)

@@ -35,14 +35,35 @@ struct FieldConst {
     double fscale[5];
 };
 
-// Sweep geometry: a CTA covers a kTB x kTA window of faces in the plane
-// normal to the sweep and marches along the normal through seg_len faces.
-constexpr int kTB = 16;             // window width along the first in-plane axis (threadIdx.x)
-constexpr int kTA = 8;              // window height along the second in-plane axis (threadIdx.y)
-constexpr int kWB = kTB + 2;        // window incl. one neighbour face each side
-constexpr int kWA = kTA + 2;
-constexpr int kWC = kWA * kWB;      // cells in one slab of the window
-constexpr int kSweepThreads = kTA * kTB;
+// Sweep geometry: a CTA covers a TB x TA window of faces in the plane normal
+// to the sweep and marches along the normal through seg_len faces.  Each
+// compute type has a small set of windows (with the CTAs per SM their register
+// budget targets); gkm_autotune picks the window and the segment length per
+// sweep direction by timing them on the live state.
+template <int TB_, int TA_, int CTAS_>
+struct SweepTile {
+    static constexpr int TB = TB_;           // window width along the first in-plane axis (threadIdx.x)
+    static constexpr int TA = TA_;           // window height along the second in-plane axis (threadIdx.y)
+    static constexpr int WB = TB + 2;        // window incl. one neighbour face each side
+    static constexpr int WA = TA + 2;
+    static constexpr int WC = WA * WB;       // cells in one slab of the window
+    static constexpr int threads = TA * TB;
+    static constexpr int ctas = CTAS_;
+};
+// FP64: 16 x 8 (255 registers, two 128-thread CTAs per SM) and 16 x 16 (one 256-thread CTA)
+using SweepTile64a = SweepTile<16, 8, 2>;
+using SweepTile64b = SweepTile<16, 16, 1>;
+// FP32: 16 x 8 (168 registers, three CTAs per SM)
+using SweepTile32a = SweepTile<16, 8, 3>;
+constexpr int kSweepVariants64 = 2;
+constexpr int kSweepVariants32 = 1;
+
+struct SweepShape {
+    int variant;   // window variant of the compute type
+    int TB, TA;    // its window
+    int ctas;      // CTAs per SM it targets
+};
+SweepShape sweep_shape(bool mixed, int variant);
 constexpr int kRing = 6;            // slabs held: the 6-cell WENO stencil
 constexpr int kSlabComps = 6;       // rho, rho u, rho v, rho w, rho E, T
 
@@ -59,9 +80,10 @@ struct SweepArgs {
 
 // kernel launchers (sweep.cu); sweep_prepare sets the sweep kernels' shared-memory limit once
 cudaError_t sweep_prepare();
-cudaError_t launch_sweep(int dir, const SweepArgs& a, int nseg, cudaStream_t s);
+cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s);
 // the same sweeps with the reconstruction and the flux in single precision (sweep_mixed.cu)
-cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, int nseg, cudaStream_t s);
+cudaError_t launch_sweep_mixed(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s);
+cudaError_t sweep_mixed_prepare();
 cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, cudaStream_t s);
 cudaError_t launch_wave_reduce(const double* W, const FieldConst& fc, DevClock* clock, int slot, cudaStream_t s);
 cudaError_t launch_flux_faces(const double* in, long long nfaces, double gam, int K, double dt, double dx,

@@ -29,6 +29,16 @@
 #define GKM_HD inline
 #endif
 
+// Code shape of the flux: both half-Maxwellian sides unrolled (one copy of the
+// side code per side) or one loop body.
+#ifndef GKM_UNROLL_SIDES
+#define GKM_UNROLL_SIDES 1
+#endif
+// Dot products of the moment contractions summed pairwise (shorter dependency chains).
+#ifndef GKM_TREE_SUMS
+#define GKM_TREE_SUMS 0
+#endif
+
 namespace gkm {
 
 constexpr double kR = 287.0;        // gas constant, src/param.h:21
@@ -121,12 +131,27 @@ GKM_HD T face_energy(T r, T m1, T m2, T m3, T Tf, const Phys<T>& ph)
 // Maxwellian moments of one state: x half-space table H (and H2 for the
 // equilibrium state's other half), full tables X (x), Y (y), Z (z).
 // src/GKMflux.cpp:45-68 (l, r) and :85-103 (e).
+// The tangential tables enter the moments only as products Y[b] Z[c] with
+// b + c <= 5, so they are kept as that 21-entry product table: every triple
+// product of MCal then costs one multiplication instead of two.
+// (GKM_SHARED_YZ 0 keeps the separate tables and forms every triple product
+// with two multiplications as the reference's MCal does; the operation counter
+// uses that to count the reference formulation.)
+#ifndef GKM_SHARED_YZ
+#define GKM_SHARED_YZ 1
+#endif
+constexpr int kYZ = 21;
+GKM_HD constexpr int yz(int b, int c) { return 6 * c - c * (c - 1) / 2 + b; }
+
 template <class T>
 struct Moments {
     T H[7];
     T X[7];
-    T Y[6];
-    T Z[6];
+#if GKM_SHARED_YZ
+    T YZ[kYZ];
+#else
+    T Y[6], Z[6];
+#endif
     T Ie2, Ie4;
 };
 
@@ -184,17 +209,36 @@ GKM_HD void build_moments(Moments<T>& M, const T U[3], T lam, int K, int half)
     M.Ie4 = T(3 * K + K * (K - 1)) * inv2lam * inv2lam;
     half_table<T>(M.H, U[0], lam, inv2lam, half);
     full_table<T, 7>(M.X, U[0], inv2lam);
+#if GKM_SHARED_YZ
+    T Y[6], Z[6];
+    full_table<T, 6>(Y, U[1], inv2lam);
+    full_table<T, 6>(Z, U[2], inv2lam);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+#pragma unroll
+        for (int b = 0; b + c < 6; b++) M.YZ[yz(b, c)] = Y[b] * Z[c];
+#else
     full_table<T, 6>(M.Y, U[1], inv2lam);
     full_table<T, 6>(M.Z, U[2], inv2lam);
+#endif
 }
+
+#if GKM_SHARED_YZ
+#define GKM_TABLES(S) S.YZ
+#define TM(A, B, C) (I[k + (A)] * YZ[yz(l + (B), m + (C))])
+#define GKM_YZ_PARAM const T* YZ
+#else
+#define GKM_TABLES(S) S.Y, S.Z
+#define TM(A, B, C) (I[k + (A)] * Y[l + (B)] * Z[m + (C)])
+#define GKM_YZ_PARAM const T* Y, const T* Z
+#endif
 
 // ----------------------------------------------------------- MCal -----
 // <psi (u^k v^l w^m) (a0 + a1 u + a2 v + a3 w + a4 psi4)> with psi = (1,u,v,w,psi4),
 // psi4 = (u^2+v^2+w^2+xi^2)/2; I = normal table (full or half), Y, Z tangential.
 template <int k, int l, int m, class T>
-GKM_HD void mcal(T M[5], const T* I, const T* Y, const T* Z, T Ie2, T Ie4, const T a[5])
+GKM_HD void mcal(T M[5], const T* I, GKM_YZ_PARAM, T Ie2, T Ie4, const T a[5])
 {
-#define TM(A, B, C) (I[k + (A)] * Y[l + (B)] * Z[m + (C)])
     T t000 = TM(0, 0, 0), t100 = TM(1, 0, 0), t010 = TM(0, 1, 0), t001 = TM(0, 0, 1);
     T t200 = TM(2, 0, 0), t020 = TM(0, 2, 0), t002 = TM(0, 0, 2);
     T t110 = TM(1, 1, 0), t101 = TM(1, 0, 1), t011 = TM(0, 1, 1);
@@ -202,27 +246,31 @@ GKM_HD void mcal(T M[5], const T* I, const T* Y, const T* Z, T Ie2, T Ie4, const
     T v1 = T(0.5) * (TM(3, 0, 0) + TM(1, 2, 0) + TM(1, 0, 2) + t100 * Ie2);
     T v2 = T(0.5) * (TM(2, 1, 0) + TM(0, 3, 0) + TM(0, 1, 2) + t010 * Ie2);
     T v3 = T(0.5) * (TM(2, 0, 1) + TM(0, 2, 1) + TM(0, 0, 3) + t001 * Ie2);
+#if GKM_TREE_SUMS
+    M[0] = (a[0] * t000 + a[1] * t100) + (a[2] * t010 + a[3] * t001) + a[4] * v0;
+    M[1] = (a[0] * t100 + a[1] * t200) + (a[2] * t110 + a[3] * t101) + a[4] * v1;
+    M[2] = (a[0] * t010 + a[1] * t110) + (a[2] * t020 + a[3] * t011) + a[4] * v2;
+    M[3] = (a[0] * t001 + a[1] * t101) + (a[2] * t011 + a[3] * t002) + a[4] * v3;
+#else
     M[0] = a[0] * t000 + a[1] * t100 + a[2] * t010 + a[3] * t001 + a[4] * v0;
     M[1] = a[0] * t100 + a[1] * t200 + a[2] * t110 + a[3] * t101 + a[4] * v1;
     M[2] = a[0] * t010 + a[1] * t110 + a[2] * t020 + a[3] * t011 + a[4] * v2;
     M[3] = a[0] * t001 + a[1] * t101 + a[2] * t011 + a[3] * t002 + a[4] * v3;
+#endif
     M[4] = T(0.25) * a[4] *
                (TM(4, 0, 0) + TM(0, 4, 0) + TM(0, 0, 4) + t000 * Ie4 +
                 T(2) * (TM(2, 2, 0) + TM(2, 0, 2) + t200 * Ie2 + TM(0, 2, 2) + t020 * Ie2 + t002 * Ie2)) +
            a[0] * v0 + a[1] * v1 + a[2] * v2 + a[3] * v3;
-#undef TM
 }
 
 template <int k, int l, int m, class T>
-GKM_HD void mcal0(T M[5], const T* I, const T* Y, const T* Z, T Ie2)
+GKM_HD void mcal0(T M[5], const T* I, GKM_YZ_PARAM, T Ie2)
 {
-#define TM(A, B, C) (I[k + (A)] * Y[l + (B)] * Z[m + (C)])
     M[0] = TM(0, 0, 0);
     M[1] = TM(1, 0, 0);
     M[2] = TM(0, 1, 0);
     M[3] = TM(0, 0, 1);
     M[4] = T(0.5) * (TM(2, 0, 0) + TM(0, 2, 0) + TM(0, 0, 2) + TM(0, 0, 0) * Ie2);
-#undef TM
 }
 
 template <class T>
@@ -374,7 +422,11 @@ GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[
 
     const T cB = gm4 + gm5;
     // ---------------- one side (l: positive half with left state, r: negative half with right state)
+#if GKM_UNROLL_SIDES
 #pragma unroll
+#else
+#pragma unroll 1
+#endif
     for (int side = 0; side < 2; side++) {
         const T den = side == 0 ? denl : denr;
         const T* Us = side == 0 ? Ul : Ur;
@@ -383,7 +435,7 @@ GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[
         build_moments<T>(S, Us, lam, K, side == 0 ? +1 : -1);
         SlopeState<T> ss = slope_state<T>(Us, lam, K);
         T iden = T(1) / den;
-        mcal0<0, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2);
+        mcal0<0, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2);
         axpy5<T>(We, den, M);
         T Bs[5] = {0, 0, 0, 0, 0};   // -(Mf100 ax + Mf010 ay + Mf001 az)
         T b[5], a[5];
@@ -391,44 +443,44 @@ GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[
 #pragma unroll
         for (int q = 0; q < 5; q++) b[q] = in.DW(0 + side, q) * iden;
         slope_solve<T>(b, ss, a);
-        mcal<1, 0, 0, T>(M, S.X, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<1, 0, 0, T>(M, S.X, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Bs, T(-1), M);
-        mcal<1, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<1, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Bacc, cB * den, M);
-        mcal<2, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<2, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Facc, p4 * den, M);
         // first tangential slope
 #pragma unroll
         for (int q = 0; q < 5; q++) b[q] = in.DW(2 + side, q) * iden;
         slope_solve<T>(b, ss, a);
-        mcal<0, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<0, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(by_, T(1), M);
-        mcal<0, 1, 0, T>(M, S.X, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<0, 1, 0, T>(M, S.X, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Bs, T(-1), M);
-        mcal<0, 1, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<0, 1, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Bacc, cB * den, M);
-        mcal<1, 1, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<1, 1, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Facc, p4 * den, M);
         // second tangential slope
 #pragma unroll
         for (int q = 0; q < 5; q++) b[q] = in.DW(4 + side, q) * iden;
         slope_solve<T>(b, ss, a);
-        mcal<0, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<0, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(bz_, T(1), M);
-        mcal<0, 0, 1, T>(M, S.X, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<0, 0, 1, T>(M, S.X, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Bs, T(-1), M);
-        mcal<0, 0, 1, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<0, 0, 1, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Bacc, cB * den, M);
-        mcal<1, 0, 1, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<1, 0, 1, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Facc, p4 * den, M);
         // time slope of this side, src/GKMflux.cpp:145-151
         slope_solve<T>(Bs, ss, a);
-        mcal<0, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<0, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Bacc, gm5 * den, M);
-        mcal<1, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2, S.Ie4, a);
+        mcal<1, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2, S.Ie4, a);
         axpy5<T>(Facc, p5 * den, M);
         // free transport of the initial half-Maxwellian
-        mcal0<1, 0, 0, T>(M, S.H, S.Y, S.Z, S.Ie2);
+        mcal0<1, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2);
         axpy5<T>(Facc, p3 * den, M);
     }
 
@@ -450,37 +502,37 @@ GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[
 #pragma unroll
     for (int q = 0; q < 5; q++) b[q] = (We[q] - in.WL(q)) * idx2;
     slope_solve<T>(b, se, a);
-    mcal<1, 0, 0, T>(M, E.H, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<1, 0, 0, T>(M, E.H, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Bacc, gm2 * dene, M);
-    mcal<2, 0, 0, T>(M, E.H, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<2, 0, 0, T>(M, E.H, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Facc, p2 * dene, M);
 #pragma unroll
     for (int q = 0; q < 5; q++) b[q] = (in.WR(q) - We[q]) * idx2;
     slope_solve<T>(b, se, a);
-    mcal<1, 0, 0, T>(M, H2, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<1, 0, 0, T>(M, H2, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Bacc, gm2 * dene, M);
-    mcal<2, 0, 0, T>(M, H2, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<2, 0, 0, T>(M, H2, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Facc, p2 * dene, M);
     // tangential equilibrium slopes
     slope_solve<T>(by_, se, a);
-    mcal<0, 1, 0, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<0, 1, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Bacc, gm2 * dene, M);
-    mcal<1, 1, 0, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<1, 1, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Facc, p2 * dene, M);
     slope_solve<T>(bz_, se, a);
-    mcal<0, 0, 1, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<0, 0, 1, T>(M, E.X, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Bacc, gm2 * dene, M);
-    mcal<1, 0, 1, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<1, 0, 1, T>(M, E.X, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Facc, p2 * dene, M);
     // time derivative of the equilibrium, src/GKMflux.cpp:183-191
-    mcal0<0, 0, 0, T>(M, E.X, E.Y, E.Z, E.Ie2);
+    mcal0<0, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
     T idene = T(1) / dene;
 #pragma unroll
     for (int q = 0; q < 5; q++) b[q] = (gm1 * dene * M[q] + Bacc[q] + gm3 * We[q]) * idene;
     slope_solve<T>(b, se, a);
-    mcal<1, 0, 0, T>(M, E.X, E.Y, E.Z, E.Ie2, E.Ie4, a);
+    mcal<1, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2, E.Ie4, a);
     axpy5<T>(Facc, p1 * dene, M);
-    mcal0<1, 0, 0, T>(M, E.X, E.Y, E.Z, E.Ie2);
+    mcal0<1, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
     axpy5<T>(Facc, p0 * dene, M);
 #pragma unroll
     for (int q = 0; q < 5; q++) F[q] = Facc[q];

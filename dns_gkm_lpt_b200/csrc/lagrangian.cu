@@ -106,15 +106,134 @@ __global__ void spline_pass1(const double* __restrict__ in, SplineGrid g, Spline
     }
 }
 
-// pass 2: [M0][M1][N2] along axis 2 -> [M0][M1][M2]
-__global__ void spline_pass2(const double* __restrict__ in, SplineGrid g, SplineTables tb, double* __restrict__ out)
+// pass 2: [M0][M1][N2] along axis 2 -> [M0][M1][M2].  Lines are contiguous,
+// so a thread per line would read 32 scattered addresses per warp access.
+// Instead each warp owns 32 lines and moves 32-value chunks of them through
+// shared memory (coalesced 256 B rows); lane j then runs line j's recurrence on
+// its staged row.  The arithmetic per line is the one of line_solve, in the
+// same order, so the coefficients are identical.
+constexpr int kLineChunk = 32;
+constexpr int kPass2Warps = 4;
+
+__global__ void __launch_bounds__(32 * kPass2Warps) spline_pass2(const double* __restrict__ in, SplineGrid g,
+                                                                 SplineTables tb, double* __restrict__ out)
 {
+    __shared__ double stage[kPass2Warps][32][kLineChunk + 1];
     const int N = g.npts, M = N + g.pad;
     const long long lines = (long long)M * M;
-    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x) {
-        const double* src = in + L * N;
-        auto f = [&](int k) { return src[k]; };
-        line_solve(f, N, g.periodic, tb, out + L * M, 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double(*sm)[kLineChunk + 1] = stage[warp];
+    const long long nwarps = (long long)gridDim.x * kPass2Warps;
+    for (long long L0 = ((long long)blockIdx.x * kPass2Warps + warp) * 32; L0 < lines; L0 += nwarps * 32) {
+        const int nl = (int)min(32LL, lines - L0);           // lines of this warp
+        const long long myL = L0 + lane;
+        const bool mine = lane < nl;
+        // load chunk [k0, k0+kLineChunk) of the warp's lines into sm[j][t]
+        auto load = [&](const double* base, long long stride, int k0, int off) {
+            for (int j = 0; j < nl; j++) {
+                const int k = k0 + lane;
+                if (k < N) sm[j][lane] = base[(L0 + j) * stride + k + off];
+            }
+            __syncwarp();
+        };
+        auto store = [&](double* base, long long stride, int k0, int off, int kmax) {
+            __syncwarp();
+            for (int j = 0; j < nl; j++) {
+                const int k = k0 + lane;
+                if (k < kmax) base[(L0 + j) * stride + k + off] = sm[j][lane];
+            }
+            __syncwarp();
+        };
+        const double* src = in + myL * N;
+        double* dst = out + myL * M;
+        if (!g.periodic) {
+            const double c0 = mine ? src[0] : 0.0, cl = mine ? src[N - 1] : 0.0;
+            // forward elimination: slot i+1 <- rp_i for i = 1..N-2 (chunks of i)
+            double rp = 0.0;
+            for (int k0 = 0; k0 < N; k0 += kLineChunk) {
+                load(in, N, k0, 0);
+                if (mine)
+                    for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
+                        const int i = k0 + t;
+                        if (i < 1 || i > N - 2) continue;
+                        double r = mul(6.0, sm[lane][t]);
+                        if (i == 1) r = sub(r, c0);
+                        if (i == N - 2) r = sub(r, cl);
+                        rp = (i == 1) ? r : sub(r, mul(tb.mt[i], rp));
+                        sm[lane][t] = rp;
+                    }
+                store(out, M, k0, 1, N);   // value of i lands in slot i+1
+            }
+            // back substitution, chunks in descending order
+            double x = 0.0, x1 = 0.0, xl2 = 0.0;
+            for (int k0 = ((N - 1) / kLineChunk) * kLineChunk; k0 >= 0; k0 -= kLineChunk) {
+                load(out, M, k0, 1);
+                if (mine)
+                    for (int t = kLineChunk - 1; t >= 0; t--) {
+                        const int i = k0 + t;
+                        if (i < 1 || i > N - 2) continue;
+                        x = (i == N - 2) ? __ddiv_rn(sm[lane][t], tb.dp[N - 2])
+                                         : __ddiv_rn(sub(sm[lane][t], x), tb.dp[i]);
+                        sm[lane][t] = x;
+                        if (i == N - 2) xl2 = x;
+                        if (i == 1) x1 = x;
+                    }
+                store(out, M, k0, 1, N);
+            }
+            if (mine) {
+                dst[1] = c0;
+                dst[N] = cl;
+                dst[0] = sub(2.0 * c0, x1);
+                dst[N + 1] = sub(2.0 * cl, xl2);
+            }
+        } else {
+            double rp = 0.0;
+            for (int k0 = 0; k0 < N; k0 += kLineChunk) {
+                load(in, N, k0, 0);
+                if (mine)
+                    for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
+                        const int i = k0 + t;
+                        rp = (i == 0) ? mul(6.0, sm[lane][t]) : sub(mul(6.0, sm[lane][t]), mul(tb.mt[i], rp));
+                        sm[lane][t] = rp;
+                    }
+                store(out, M, k0, 1, N);
+            }
+            double x = 0.0, x0 = 0.0, xl = 0.0;
+            for (int k0 = ((N - 1) / kLineChunk) * kLineChunk; k0 >= 0; k0 -= kLineChunk) {
+                load(out, M, k0, 1);
+                if (mine)
+                    for (int t = kLineChunk - 1; t >= 0; t--) {
+                        const int i = k0 + t;
+                        if (i > N - 1) continue;
+                        x = (i == N - 1) ? __ddiv_rn(sm[lane][t], tb.dp[N - 1])
+                                         : __ddiv_rn(sub(sm[lane][t], x), tb.dp[i]);
+                        sm[lane][t] = x;
+                        if (i == N - 1) xl = x;
+                        if (i == 0) x0 = x;
+                    }
+                store(out, M, k0, 1, N);
+            }
+            const double fac = mine ? __ddiv_rn(add(x0, mul(-0.25, xl)), tb.denom) : 0.0;
+            double y0 = 0.0, y1 = 0.0, yl = 0.0;
+            for (int k0 = 0; k0 < N; k0 += kLineChunk) {
+                load(out, M, k0, 1);
+                if (mine)
+                    for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
+                        const int i = k0 + t;
+                        const double v = sub(sm[lane][t], mul(fac, tb.z[i]));
+                        sm[lane][t] = v;
+                        if (i == 0) y0 = v;
+                        if (i == 1) y1 = v;
+                        if (i == N - 1) yl = v;
+                    }
+                store(out, M, k0, 1, N);
+            }
+            if (mine) {
+                dst[0] = yl;
+                dst[N + 1] = y0;
+                dst[N + 2] = y1;
+            }
+        }
     }
 }
 
@@ -366,6 +485,16 @@ cudaError_t grid_launch(K kernel, long long work, int threads, cudaStream_t s, A
     return cudaGetLastError();
 }
 
+cudaError_t launch_pass2(const double* in, const SplineGrid& g, const SplineTables& tb, double* out, cudaStream_t s)
+{
+    const long long M = g.npts + g.pad;
+    long long b = (M * M + 32 * kPass2Warps - 1) / (32 * kPass2Warps);
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    spline_pass2<<<(unsigned)b, 32 * kPass2Warps, 0, s>>>(in, g, tb, out);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t launch_spline_build(const double* W, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
@@ -378,7 +507,7 @@ cudaError_t launch_spline_build(const double* W, const FieldConst& fc, const Spl
         if (e != cudaSuccess) return e;
         e = grid_launch(spline_pass1, M * N, 128, s, (const double*)outs[f], g, tb, scratch);
         if (e != cudaSuccess) return e;
-        e = grid_launch(spline_pass2, M * M, 128, s, (const double*)scratch, g, tb, outs[f]);
+        e = launch_pass2((const double*)scratch, g, tb, outs[f], s);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -393,7 +522,7 @@ cudaError_t launch_spline_component(const double* W, const FieldConst& fc, const
     if (e != cudaSuccess) return e;
     e = grid_launch(spline_pass1, M * N, 128, s, (const double*)coef, g, tb, scratch);
     if (e != cudaSuccess) return e;
-    return grid_launch(spline_pass2, M * M, 128, s, (const double*)scratch, g, tb, coef);
+    return launch_pass2((const double*)scratch, g, tb, coef, s);
 }
 
 cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np, const double* py,

@@ -1,7 +1,9 @@
 // Algorithmic operation count of one cell update, taken from the device
 // numerics themselves: gkm_numerics.cuh is instantiated on the host with a
-// scalar type that counts every arithmetic operation it performs.  The count
-// is the numerator of the FP64 roofline reported by bench.py.
+// scalar type that counts every arithmetic operation it performs, in the
+// reference's formulation of the moments (GKM_SHARED_YZ 0) and with one
+// reconstruction per face.  The count is the numerator of the FP64 roofline
+// reported by bench.py, so it stays fixed when the kernels get cheaper.
 //
 // Per face (one reconstruction per face, as the sweep kernels do):
 //   temperature of the cell entering the stencil window  1x
@@ -40,6 +42,10 @@ inline bool operator<(Num a, Num b) { g_cnt.cmp++; return a.v < b.v; }
 inline Num fabs(Num a) { return Num(std::fabs(a.v)); }
 inline Num fmax(Num a, Num b) { g_cnt.cmp++; return Num(std::fmax(a.v, b.v)); }
 
+// count the gas-kinetic moments as the reference's MCal forms them
+// (src/GKMflux.cpp:238-278: two multiplications per triple product); the
+// kernels share the Y*Z products and execute fewer
+#define GKM_SHARED_YZ 0
 #include "gkm_numerics.cuh"
 
 namespace gkm {
@@ -162,7 +168,7 @@ int main()
     addc(cell, acc, 1);
     addc(cell, wave, 1);
 
-    std::printf("{\n  \"what\": \"FP64 operations of one cell update (three faces) in the sweep kernels' formulation\",\n");
+    std::printf("{\n  \"what\": \"FP64 operations of one cell update (three faces): reference formulation of the moments, one reconstruction per face\",\n");
     std::printf("  \"per_call\": {\n");
     print("temperature", c_temp, ",");
     print("weno_scalar_both_sides", c_weno1, ",");

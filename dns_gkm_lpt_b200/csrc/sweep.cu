@@ -139,33 +139,54 @@ __global__ void weno_faces_kernel(const double* __restrict__ s, long long n, Phy
     }
 }
 
-template <int DIR>
+template <int DIR, class Tile>
 cudaError_t launch_one(const SweepArgs& a, int nseg, cudaStream_t s)
 {
-    dim3 grid((a.fc.n + kTB - 1) / kTB, (a.fc.n + kTA - 1) / kTA, nseg);
-    dim3 block(kTB, kTA);
-    sweep_kernel<DIR, double><<<grid, block, sweep_detail::sweep_smem_bytes<double>(), s>>>(a);
+    dim3 grid((a.fc.n + Tile::TB - 1) / Tile::TB, (a.fc.n + Tile::TA - 1) / Tile::TA, nseg);
+    dim3 block(Tile::TB, Tile::TA);
+    sweep_kernel<DIR, double, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<double, Tile>(), s>>>(a);
     return cudaGetLastError();
+}
+
+template <class Tile>
+cudaError_t set_smem()
+{
+    const int bytes = (int)sweep_detail::sweep_smem_bytes<double, Tile>();
+    cudaError_t e =
+        cudaFuncSetAttribute(sweep_kernel<0, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_kernel<1, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_kernel<2, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
 }
 
 }  // namespace
 
 cudaError_t sweep_prepare()
 {
-    const int bytes = (int)sweep_detail::sweep_smem_bytes<double>();
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = set_smem<SweepTile64a>();
+    if (e == cudaSuccess) e = set_smem<SweepTile64b>();
     return e;
 }
 
-cudaError_t launch_sweep(int dir, const SweepArgs& a, int nseg, cudaStream_t s)
+SweepShape sweep_shape(bool mixed, int variant)
 {
-    if (dir == 0) return launch_one<0>(a, nseg, s);
-    if (dir == 1) return launch_one<1>(a, nseg, s);
-    return launch_one<2>(a, nseg, s);
+    if (mixed) return {0, SweepTile32a::TB, SweepTile32a::TA, SweepTile32a::ctas};
+    if (variant == 1) return {1, SweepTile64b::TB, SweepTile64b::TA, SweepTile64b::ctas};
+    return {0, SweepTile64a::TB, SweepTile64a::TA, SweepTile64a::ctas};
+}
+
+cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s)
+{
+    if (variant == 1) {
+        if (dir == 0) return launch_one<0, SweepTile64b>(a, nseg, s);
+        if (dir == 1) return launch_one<1, SweepTile64b>(a, nseg, s);
+        return launch_one<2, SweepTile64b>(a, nseg, s);
+    }
+    if (dir == 0) return launch_one<0, SweepTile64a>(a, nseg, s);
+    if (dir == 1) return launch_one<1, SweepTile64a>(a, nseg, s);
+    return launch_one<2, SweepTile64a>(a, nseg, s);
 }
 
 cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, cudaStream_t s)

@@ -53,7 +53,7 @@ struct Neigh {
     static constexpr double ys = DIR == 1 ? -0.5 : 0.5;
 };
 
-template <int DIR, class T>
+template <int DIR, class T, int kWC>
 struct SmemFace {
     const T* __restrict__ wf;   // slab of the left cell (6 comps x kWC)
     const T* __restrict__ wf1;  // slab of the right cell
@@ -118,23 +118,20 @@ __device__ __forceinline__ double block_max(double v, double* red)
     return v;
 }
 
-template <class T>
+template <class T, class Tile>
 constexpr size_t sweep_smem_bytes()
 {
-    return sizeof(T) * (size_t)(kRing * kSlabComps * kWC + 10 * kWC);
+    return sizeof(T) * (size_t)(kRing * kSlabComps * Tile::WC + 10 * Tile::WC);
 }
-
-template <class T>
-struct SweepOccupancy {
-    static constexpr int ctas = sizeof(T) == 8 ? 2 : 3;   // CTAs of 128 threads per SM the registers allow
-};
 
 }  // namespace sweep_detail
 
-template <int DIR, class T>
-__global__ void __launch_bounds__(kSweepThreads, sweep_detail::SweepOccupancy<T>::ctas) sweep_kernel(SweepArgs a)
+template <int DIR, class T, class Tile>
+__global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepArgs a)
 {
     using namespace sweep_detail;
+    constexpr int kTB = Tile::TB, kTA = Tile::TA, kWB = Tile::WB, kWC = Tile::WC;
+    constexpr int kSweepThreads = Tile::threads;
     constexpr bool kMixed = sizeof(T) == 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ring = reinterpret_cast<T*>(smem_raw);          // [kRing][kSlabComps][kWC]
@@ -238,7 +235,7 @@ __global__ void __launch_bounds__(kSweepThreads, sweep_detail::SweepOccupancy<T>
         }
         __syncthreads();
         if (active) {
-            SmemFace<DIR, T> pv;
+            SmemFace<DIR, T, kWC> pv;
             pv.wf = slot(f);
             pv.wf1 = slot(f + 1);
             pv.rec = rec;

@@ -5,8 +5,10 @@
 // update in FP64, exactly as the FP64 sweeps accumulate them.
 //
 // Compiled with fast single-precision math (-use_fast_math: approximate
-// division, square root and exp, denormals flushed); the FP64 arithmetic of
-// this file is unaffected by that flag.
+// division, square root and exp, denormals flushed; the FP64 arithmetic of
+// this file is unaffected by that flag) and with the flux's two half-Maxwellian
+// sides as one loop body (-DGKM_UNROLL_SIDES=0), the faster code shape for
+// the single-precision flux.
 #include "sweep_impl.cuh"
 
 namespace gkm {
@@ -15,16 +17,31 @@ namespace {
 template <int DIR>
 cudaError_t launch_one_mixed(const SweepArgs& a, int nseg, cudaStream_t s)
 {
-    dim3 grid((a.fc.n + kTB - 1) / kTB, (a.fc.n + kTA - 1) / kTA, nseg);
-    dim3 block(kTB, kTA);
-    sweep_kernel<DIR, float><<<grid, block, sweep_detail::sweep_smem_bytes<float>(), s>>>(a);
+    using Tile = SweepTile32a;
+    dim3 grid((a.fc.n + Tile::TB - 1) / Tile::TB, (a.fc.n + Tile::TA - 1) / Tile::TA, nseg);
+    dim3 block(Tile::TB, Tile::TA);
+    sweep_kernel<DIR, float, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<float, Tile>(), s>>>(a);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, int nseg, cudaStream_t s)
+cudaError_t sweep_mixed_prepare()
 {
+    using Tile = SweepTile32a;
+    const int bytes = (int)sweep_detail::sweep_smem_bytes<float, Tile>();
+    cudaError_t e =
+        cudaFuncSetAttribute(sweep_kernel<0, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_kernel<1, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_kernel<2, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
+
+cudaError_t launch_sweep_mixed(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s)
+{
+    (void)variant;   // one window for the single-precision sweeps
     if (dir == 0) return launch_one_mixed<0>(a, nseg, s);
     if (dir == 1) return launch_one_mixed<1>(a, nseg, s);
     return launch_one_mixed<2>(a, nseg, s);

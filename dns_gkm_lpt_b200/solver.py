@@ -133,6 +133,17 @@ class Solver:
         keys = ("sweep_x", "sweep_y", "sweep_z", "halo", "splines", "particles", "total")
         return dict(zip(keys, ms.tolist()))
 
+    def autotune(self, reps: int = 2) -> list:
+        """Pick the fastest window and segment length per sweep direction on the current state."""
+        self._check(self.L.gkm_autotune(self.h, reps))
+        return self.sweep_config()
+
+    def sweep_config(self) -> list:
+        out = (C.c_int32 * 12)()
+        self._check(self.L.gkm_sweep_config(self.h, out))
+        return [{"dir": "xyz"[d], "variant": out[4 * d], "window": [out[4 * d + 1], out[4 * d + 2]],
+                 "segment": out[4 * d + 3]} for d in range(3)]
+
     def launch_count(self) -> int:
         n = C.c_int64()
         self._check(self.L.gkm_launch_count(self.h, C.byref(n)))

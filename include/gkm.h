@@ -153,6 +153,16 @@ gkm_status gkm_evolve_particles(gkm_handle* h);
  * reduction), halo wrap, spline build, particle advection, whole steps. */
 gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles, double ms[7]);
 
+/* Sweep autotuner (no counterpart in the reference, whose loops have one
+ * fixed shape): for each sweep direction, times every window variant of the
+ * handle's precision with segment lengths from n down to 8 faces along the
+ * sweep normal, `reps` launches each (CUDA events on the handle's stream), and
+ * keeps the fastest.  The state is not changed; captured graphs are rebuilt. */
+gkm_status gkm_autotune(gkm_handle* h, int32_t reps);
+/* The sweep shapes in use: for x, y, z in turn: window variant, window width,
+ * window height, segment length (faces per CTA along the normal). */
+gkm_status gkm_sweep_config(const gkm_handle* h, int32_t out[12]);
+
 /* Kernels this handle has launched so far (graph replays count their kernels). */
 gkm_status gkm_launch_count(const gkm_handle* h, int64_t* count);
 
