@@ -45,6 +45,22 @@ HBM_PEAK_GBS = 6550.7        # measured copy bandwidth of this pool's B200s
 SWEEP_DRAM_BYTES_PER_CELL = 102.8   # profiles/sweep_kernel_fp64_128cube_full.md, mean of x/y/z
 
 
+# batched ensemble: 16 x 32^3 + 8 x 48^3 + 6 x 64^3 + 2 x 96^3 (4.75 M cells), Mt ~ U[0.1, 0.6],
+# Re_lambda ~ U[20, 80], 10^4 particles each; member m uses seed 10000 + m
+ENSEMBLE = [(32, 16), (48, 8), (64, 6), (96, 2)]
+ENS_PART = 10_000
+
+
+def ensemble_specs():
+    import numpy as np
+    rng = np.random.default_rng(10000)
+    specs = []
+    for n, count in ENSEMBLE:
+        for _ in range(count):
+            specs.append((n, float(rng.uniform(0.1, 0.6)), float(rng.uniform(20.0, 80.0)), 10000 + len(specs)))
+    return specs
+
+
 def cells_of(n: int) -> int:
     return n ** 3
 
@@ -148,6 +164,108 @@ def reference_arm(args, world: int):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------ batched ensemble --
+def _rel_l2(a, b):
+    import numpy as np
+    sl = slice(3, -3)
+    return max(float(np.linalg.norm(a[q, sl, sl, sl] - b[q, sl, sl, sl]) / np.linalg.norm(b[q, sl, sl, sl]))
+               for q in range(5))
+
+
+def batched_forms(args, local_rank: int, stream):
+    """C4 ensemble in FP64 and mixed precision (one launch per stage, graph-captured
+    step) against the same members stepped one after another as single cubes."""
+    import torch
+
+    from dns_gkm_lpt_b200 import ic
+    from dns_gkm_lpt_b200.solver import Ensemble, Solver
+
+    specs = ensemble_specs()
+    inputs = []
+    for n, Mt, Re, seed in specs:
+        P, u, v, w, rho, p = ic.make_field(n, Mt, Re, seed)
+        inputs.append((P, ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, p)),
+                       ic.particles_to_reference_order(ic.make_particles(ENS_PART, seed))))
+    cells = sum(n ** 3 for n, _, _, _ in specs)
+    steps = args.steps
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def eul(ph):
+        return ph["sweep_x"] + ph["sweep_y"] + ph["sweep_z"] + ph["halo"]
+
+    def run_ensemble(precision):
+        E = Ensemble([{"params": P, "cfl": CFL, "max_particles": ENS_PART} for P, _, _ in inputs],
+                     device=local_rank, precision=precision)
+        for m, (_, W0, pos) in enumerate(inputs):
+            E[m].upload_state(W0)
+            E[m].particles_upload(pos)
+        cfg = E.autotune(2)
+        E.step_timed(args.warmup)
+        ph = E.step_timed(steps)
+        st = torch.cuda.ExternalStream(E.stream())
+        E.step(1)                                  # graph instantiation, untimed
+        l0 = E.launch_count()
+        ev[0].record(st)
+        E.step(steps)
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        graph_ms = ev[0].elapsed_time(ev[1])
+        launches = E.launch_count() - l0
+        states = [E[m].download_state() for m in range(len(E))]
+        tke = [E[m].print_stats()["TKE"] for m in range(len(E))]
+        E.close()
+        return ph, graph_ms, launches, cfg, states, tke
+
+    def run_sequential():
+        ph_sum, graph_ms, states = {}, 0.0, []
+        for P, W0, pos in inputs:
+            s = Solver(P, cfl=CFL, max_particles=ENS_PART, device=local_rank)
+            s.set_stream(stream.cuda_stream)
+            s.upload_state(W0)
+            s.particles_upload(pos)
+            s.autotune(1)
+            s.step_timed(args.warmup, True)
+            ph = s.step_timed(steps, True)
+            for k, v in ph.items():
+                ph_sum[k] = ph_sum.get(k, 0.0) + v
+            s.step(1)
+            ev[0].record(stream)
+            s.step(steps)
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+            graph_ms += ev[0].elapsed_time(ev[1])
+            states.append(s.download_state())
+            s.close()
+        return ph_sum, graph_ms, states
+
+    out = {}
+    ph64, g64, l64, cfg64, W64, tke64 = run_ensemble(0)
+    phs, gs, Ws = run_sequential()
+    members = " + ".join(f"{c} x {n}^3" for n, c in ENSEMBLE)
+    common = {"members": members, "cells": cells, "particles_per_member": ENS_PART}
+    out["batched_fp64"] = dict(common, **{
+        "value": cells * steps / (eul(ph64) * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+        "particle_steps_per_s": len(specs) * ENS_PART * steps / ((ph64["splines"] + ph64["particles"]) * 1e-3),
+        "graph_ms_per_step": g64 / steps, "graph_launches_per_step": l64 / steps,
+        "sequential_single_cubes": {"value": cells * steps / (eul(phs) * 1e-3) / 1e9,
+                                    "graph_ms_per_step": gs / steps,
+                                    "what": "same members, one handle each, stepped one after another"},
+        "speedup_vs_sequential_graph": gs / g64,
+        "max_rel_l2_vs_single_cubes": max(_rel_l2(a, b) for a, b in zip(W64, Ws)),
+        "sweep_shapes": cfg64})
+    del Ws
+    phm, gm, lm, cfgm, Wm, tkem = run_ensemble(1)
+    out["batched_mixed"] = dict(common, **{
+        "value": cells * steps / (eul(phm) * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+        "particle_steps_per_s": len(specs) * ENS_PART * steps / ((phm["splines"] + phm["particles"]) * 1e-3),
+        "graph_ms_per_step": gm / steps, "graph_launches_per_step": lm / steps,
+        "speedup_vs_sequential_graph": gs / gm,
+        "max_rel_l2_vs_fp64": max(_rel_l2(a, b) for a, b in zip(Wm, W64)),
+        "max_tke_rel_err_vs_fp64": max(abs(a - b) / b for a, b in zip(tkem, tke64)),
+        "steps_compared": args.warmup + 2 * steps + 1, "sweep_shapes": cfgm})
+    return out
+
+
 # ------------------------------------------------------------- our arm ----
 def ours(args, rank: int, world: int, local_rank: int):
     import numpy as np
@@ -225,6 +343,7 @@ def ours(args, rank: int, world: int, local_rank: int):
                           "tke_rel_err_vs_fp64": abs(tkem - tke64) / tke64,
                           "steps_compared": args.warmup + args.steps, "sweep_shapes": m_cfg}
         del W64, Wm
+        forms.update(batched_forms(args, local_rank, stream))
 
     # end to end through the plug point evolve(W, dt): pinned host W in, one step, W out
     Wh = torch.empty((5, nt, nt, nt), dtype=torch.float64, pin_memory=True)
@@ -303,7 +422,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_CELLS)
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-forms", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed-precision and batched forms")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -25,6 +25,9 @@ EXPORTS = [
     "gkm_generate_splines", "gkm_spline_coefs", "gkm_stats_compute", "gkm_flux_faces", "gkm_weno_faces",
     "gkm_set_stream", "gkm_device_state", "gkm_evolve_particles", "gkm_step_timed", "gkm_launch_count",
     "gkm_probe_fma_peak", "gkm_spline_build_noalloc", "gkm_autotune", "gkm_sweep_config",
+    "gkm_ensemble_create", "gkm_ensemble_destroy", "gkm_ensemble_last_error", "gkm_ensemble_size",
+    "gkm_ensemble_member", "gkm_ensemble_step", "gkm_ensemble_step_timed", "gkm_ensemble_autotune",
+    "gkm_ensemble_sweep_config", "gkm_ensemble_launch_count", "gkm_ensemble_synchronize", "gkm_ensemble_stream",
 ]
 
 
@@ -90,8 +93,22 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.gkm_autotune.argtypes = [_h, C.c_int32]
     L.gkm_sweep_config.argtypes = [_h, C.POINTER(C.c_int32)]
     L.gkm_spline_build_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
+    L.gkm_ensemble_create.argtypes = [C.POINTER(GkmConfig), C.c_int32, C.POINTER(_h)]
+    L.gkm_ensemble_destroy.argtypes = [_h]
+    L.gkm_ensemble_last_error.argtypes = [_h]
+    L.gkm_ensemble_last_error.restype = C.c_char_p
+    L.gkm_ensemble_size.argtypes = [_h]
+    L.gkm_ensemble_member.argtypes = [_h, C.c_int32]
+    L.gkm_ensemble_member.restype = _h
+    L.gkm_ensemble_step.argtypes = [_h, C.c_int32, C.c_int32]
+    L.gkm_ensemble_step_timed.argtypes = [_h, C.c_int32, C.c_int32, _dp]
+    L.gkm_ensemble_autotune.argtypes = [_h, C.c_int32]
+    L.gkm_ensemble_sweep_config.argtypes = [_h, C.POINTER(C.c_int32)]
+    L.gkm_ensemble_launch_count.argtypes = [_h, C.POINTER(C.c_int64)]
+    L.gkm_ensemble_synchronize.argtypes = [_h]
+    L.gkm_ensemble_stream.argtypes = [_h, C.POINTER(C.c_void_p)]
     for name in EXPORTS:
-        if name not in ("gkm_config_default", "gkm_last_error"):
+        if name not in ("gkm_config_default", "gkm_last_error", "gkm_ensemble_last_error", "gkm_ensemble_member"):
             getattr(L, name).restype = st   # gkm_status, or int for gkm_abi_version / gkm_nt
     return L
 

@@ -7,7 +7,7 @@
 // host; with use_graphs the whole step is replayed as one CUDA graph per
 // buffer parity.
 #include "gkm.h"
-#include "gkm_internal.h"
+#include "gkm_handle.h"
 
 #include <cmath>
 #include <cstdio>
@@ -17,79 +17,16 @@
 
 using gkm::DevClock;
 using gkm::FieldConst;
+using gkm_host::cuda_fail;
+using gkm_host::fail;
 
-namespace {
-constexpr int kStatsBlocks = 148 * 4;
-
-enum GraphKind { kGraphEulerian = 0, kGraphFull = 1, kGraphParticles = 2 };
-constexpr int kSplinePasses = 9;   // 3 components x 3 axes
-}  // namespace
-
-struct SweepChoice {
-    int variant = 0;   // window variant (gkm::sweep_shape)
-    int nseg = 1;      // CTAs along the sweep normal
-    int seg_len = 1;   // faces per CTA along the normal
-};
-
-struct gkm_handle {
-    gkm_config cfg{};
-    FieldConst fc{};
-    SweepChoice sweep[3];
-    cudaStream_t own_stream = nullptr, stream = nullptr;
-    double* buf[2] = {nullptr, nullptr};
-    int parity = 0;
-    DevClock* clock = nullptr;
-    bool state_loaded = false;
-    int dt_fixed_mode = 0;
-    double dt_fixed = 0.0;
-    gkm::SplineGrid grid{};
-    double* tables = nullptr;  // mt | dp | z, each npts+1
-    double denom = 0.0;
-    double* coef[3] = {nullptr, nullptr, nullptr};
-    double* scratch = nullptr;
-    bool splines_valid = false;
-    int64_t np = 0, cap = 0;
-    double* P[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // y, x, z, u, v, w
-    gkm::StatsPartial* partials = nullptr;
-    double* stats_out = nullptr;
-    cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
-    int64_t graph_np[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
-    int64_t graph_kernels[3][2] = {{0, 0}, {0, 0}, {0, 0}};
-    int64_t launches = 0;    // kernels launched (graph replays add the kernels they hold)
-    std::string err;
-};
-
-namespace {
-
-gkm_status fail(gkm_handle* h, gkm_status s, const std::string& msg)
+// Thomas tables of the spline line solves (arrays of N + 1): natural dp_1 = 4,
+// m_i = 1/dp_{i-1}, dp_i = 4 - m_i; periodic (Sherman-Morrison, gamma = -4)
+// dp_0 = 8, dp_i = b_i - m_i with b_{N-1} = 4.25, z = B^-1 (-4, 0, .., 0, 1).
+void gkm::spline_line_tables(int N, int periodic, double* mt, double* dp, double* z, double* denom)
 {
-    if (h) h->err = msg;
-    return s;
-}
-
-gkm_status cuda_fail(gkm_handle* h, cudaError_t e, const char* where)
-{
-    std::string m = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
-    return fail(h, e == cudaErrorMemoryAllocation ? GKM_ERR_NOMEM : GKM_ERR_CUDA, m);
-}
-
-#define CK(h, expr)                                         \
-    do {                                                    \
-        cudaError_t e_ = (expr);                            \
-        if (e_ != cudaSuccess) return cuda_fail(h, e_, #expr); \
-    } while (0)
-
-// Thomas tables of the spline line solves; the same recurrences as the line
-// solver's reference formulation: natural dp_1 = 4, m_i = 1/dp_{i-1},
-// dp_i = 4 - m_i; periodic (Sherman-Morrison with gamma = -4) dp_0 = 8,
-// dp_i = b_i - m_i with b_{N-1} = 4.25, z = B^-1 (-4, 0, .., 0, 1).
-void spline_tables(int N, int periodic, std::vector<double>& mt, std::vector<double>& dp, std::vector<double>& z,
-                   double& denom)
-{
-    mt.assign(N + 1, 0.0);
-    dp.assign(N + 1, 0.0);
-    z.assign(N + 1, 0.0);
-    denom = 0.0;
+    for (int i = 0; i <= N; i++) mt[i] = dp[i] = z[i] = 0.0;
+    *denom = 0.0;
     if (!periodic) {
         dp[1] = 4.0;
         for (int i = 2; i <= N - 2; i++) {
@@ -112,7 +49,25 @@ void spline_tables(int N, int periodic, std::vector<double>& mt, std::vector<dou
     }
     z[N - 1] = z[N - 1] / dp[N - 1];
     for (int i = N - 2; i >= 0; i--) z[i] = (z[i] - z[i + 1]) / dp[i];
-    denom = 1.0 + (z[0] + (-0.25) * z[N - 1]);
+    *denom = 1.0 + (z[0] + (-0.25) * z[N - 1]);
+}
+
+namespace {
+constexpr int kStatsBlocks = 148 * 4;
+
+enum GraphKind { kGraphEulerian = 0, kGraphFull = 1, kGraphParticles = 2 };
+constexpr int kSplinePasses = 9;   // 3 components x 3 axes
+}  // namespace
+
+namespace {
+
+void spline_tables(int N, int periodic, std::vector<double>& mt, std::vector<double>& dp, std::vector<double>& z,
+                   double& denom)
+{
+    mt.assign(N + 1, 0.0);
+    dp.assign(N + 1, 0.0);
+    z.assign(N + 1, 0.0);
+    gkm::spline_line_tables(N, periodic, mt.data(), dp.data(), z.data(), &denom);
 }
 
 gkm::SplineTables device_tables(const gkm_handle* h)
@@ -418,6 +373,7 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
 gkm_status gkm_destroy(gkm_handle* h)
 {
     if (!h) return GKM_ERR_ARG;
+    if (h->owner) return fail(h, GKM_ERR_STATE, "the handle belongs to an ensemble (gkm_ensemble_destroy frees it)");
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
     destroy_graphs(h);
     for (int b = 0; b < 2; b++) cudaFree(h->buf[b]);
@@ -815,6 +771,7 @@ gkm_status gkm_weno_faces(const double* stencils, int64_t n, double gam, double*
 gkm_status gkm_set_stream(gkm_handle* h, void* stream)
 {
     if (!h) return GKM_ERR_ARG;
+    if (h->owner) return fail(h, GKM_ERR_STATE, "an ensemble member runs on the ensemble's stream");
     CK(h, cudaStreamSynchronize(h->stream));
     h->stream = stream ? (cudaStream_t)stream : h->own_stream;
     destroy_graphs(h);

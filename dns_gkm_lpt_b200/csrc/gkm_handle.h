@@ -1,0 +1,67 @@
+// Host-side state of one handle, shared by the single-cube C ABI
+// (gkm_capi.cu) and the ensemble C ABI (gkm_ensemble.cu).  Not installed.
+#pragma once
+
+#include "gkm.h"
+#include "gkm_internal.h"
+
+#include <string>
+
+struct gkm_ensemble;
+
+struct SweepChoice {
+    int variant = 0;   // window variant (gkm::sweep_shape)
+    int nseg = 1;      // CTAs along the sweep normal
+    int seg_len = 1;   // faces per CTA along the normal
+};
+
+struct gkm_handle {
+    gkm_config cfg{};
+    gkm::FieldConst fc{};
+    SweepChoice sweep[3];
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    double* buf[2] = {nullptr, nullptr};
+    int parity = 0;
+    gkm::DevClock* clock = nullptr;
+    bool state_loaded = false;
+    int dt_fixed_mode = 0;
+    double dt_fixed = 0.0;
+    gkm::SplineGrid grid{};
+    double* tables = nullptr;  // mt | dp | z, each npts+1
+    double denom = 0.0;
+    double* coef[3] = {nullptr, nullptr, nullptr};
+    double* scratch = nullptr;
+    bool splines_valid = false;
+    int64_t np = 0, cap = 0;
+    double* P[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // y, x, z, u, v, w
+    gkm::StatsPartial* partials = nullptr;
+    double* stats_out = nullptr;
+    cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    int64_t graph_np[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
+    int64_t graph_kernels[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    int64_t launches = 0;    // kernels launched (graph replays add the kernels they hold)
+    std::string err;
+    gkm_ensemble* owner = nullptr;   // set while the handle is a member of an ensemble
+};
+
+namespace gkm_host {
+
+inline gkm_status fail(gkm_handle* h, gkm_status s, const std::string& msg)
+{
+    if (h) h->err = msg;
+    return s;
+}
+
+inline gkm_status cuda_fail(gkm_handle* h, cudaError_t e, const char* where)
+{
+    std::string m = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return fail(h, e == cudaErrorMemoryAllocation ? GKM_ERR_NOMEM : GKM_ERR_CUDA, m);
+}
+
+#define CK(h, expr)                                         \
+    do {                                                    \
+        cudaError_t e_ = (expr);                            \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #expr); \
+    } while (0)
+
+}  // namespace gkm_host

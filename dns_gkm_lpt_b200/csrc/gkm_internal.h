@@ -123,6 +123,60 @@ struct StatsPartial {  // per-CTA partial sums of the PrintStats moments
 cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const double* const coefs[3],
                          StatsPartial* partials, int nblocks, double* out16, cudaStream_t s);
 
+// ---------------------------------------------------------------- ensemble --
+// Independent members (own grid size, parameters, state, splines, particles)
+// advanced by shared launches: each launch walks a flattened work list whose
+// per-member prefix offsets find the member of a work index.
+struct MemberDev {
+    double* buf[2];      // state buffers (current state = buf[parity])
+    DevClock* clock;
+    FieldConst fc;
+    int dt_fixed_mode;
+    double dt_fixed;
+    int nseg[3];         // sweep segments along the normal, per direction
+    int tiles_b[3];      // windows along the first in-plane axis, per direction
+    SplineGrid grid;
+    SplineTables tb;
+    double* coef[3];
+    double* scratch[3];
+    double* P[6];        // particles y, x, z, u, v, w
+    long long np;
+};
+
+struct EnsembleWork {           // prefix offsets, nm + 1 entries each, in device memory
+    const long long* item[3];   // sweep work items per direction
+    const long long* ghost;     // ghost cells
+    const long long* line0;     // spline pass-0 lines of the 3 components
+    const long long* line1;     // spline pass-1 lines of the 3 components
+    const long long* warp2;     // spline pass-2 groups of 32 lines, 3 components
+    const long long* part;      // particles
+};
+
+// largest m with off[m] <= idx (off[0] = 0, off[nm] = total)
+__device__ __forceinline__ int find_member(const long long* __restrict__ off, int nm, long long idx)
+{
+    int lo = 0, hi = nm - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= idx) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+cudaError_t launch_ensemble_sweep64(int dir, int variant, const MemberDev* mem, const long long* off, int nm,
+                                    int parity, int seg_len, cudaStream_t s);
+cudaError_t launch_ensemble_sweep32(int dir, int variant, const MemberDev* mem, const long long* off, int nm,
+                                    int parity, int seg_len, cudaStream_t s);
+cudaError_t launch_ensemble_halo(const MemberDev* mem, const long long* off, int nm, long long total, int buf,
+                                 int finish_step, cudaStream_t s);
+cudaError_t launch_ensemble_splines(const MemberDev* mem, const EnsembleWork& w, const long long totals[3], int nm,
+                                    int buf, cudaStream_t s);
+cudaError_t launch_ensemble_heun(const MemberDev* mem, const long long* off, int nm, long long total, cudaStream_t s);
+
+// Thomas tables of the spline line solves (gkm_capi.cu)
+void spline_line_tables(int N, int periodic, double* mt, double* dp, double* z, double* denom);
+
 // FMA throughput probe (probe.cu)
 cudaError_t probe_fma_peak(double* fp64_tflops, double* fp32_tflops);
 

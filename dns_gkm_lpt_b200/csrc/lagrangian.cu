@@ -72,38 +72,49 @@ __device__ void line_solve(const Src& f, int N, int periodic, const SplineTables
     }
 }
 
-// pass 0: velocity component q of W along axis 0 (y) -> out [M0][N1][N2]
-__global__ void spline_pass0(const double* __restrict__ W, FieldConst fc, SplineGrid g, SplineTables tb, int q,
-                             double* __restrict__ out)
+// pass 0: velocity component q of W along axis 0 (y) -> out [M0][N1][N2]; one line (i, k)
+__device__ __forceinline__ void pass0_line(const double* __restrict__ W, const FieldConst& fc, const SplineGrid& g,
+                                           const SplineTables& tb, int q, double* __restrict__ out, long long L)
 {
     const int N = g.npts;
     const long long lines = (long long)N * N;
     const long long nt3 = fc.nt3;
     const int nt = fc.nt;
     const int off = g.periodic ? 3 : 0;
-    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(L / N), k = (int)(L - (long long)i * N);
-        const long long base = (long long)(i + off) * nt + (k + off);
-        const long long sj = (long long)nt * nt;
-        auto f = [&](int j) {
-            const long long idx = (long long)(j + off) * sj + base;
-            return __ddiv_rn(W[q * nt3 + idx], W[idx]);   // u = rho u / rho, src/update.cpp:1239-1241
-        };
-        line_solve(f, N, g.periodic, tb, out + L, lines);
-    }
+    const int i = (int)(L / N), k = (int)(L - (long long)i * N);
+    const long long base = (long long)(i + off) * nt + (k + off);
+    const long long sj = (long long)nt * nt;
+    auto f = [&](int j) {
+        const long long idx = (long long)(j + off) * sj + base;
+        return __ddiv_rn(W[q * nt3 + idx], W[idx]);   // u = rho u / rho, src/update.cpp:1239-1241
+    };
+    line_solve(f, N, g.periodic, tb, out + L, lines);
 }
 
-// pass 1: [M0][N1][N2] along axis 1 -> [M0][M1][N2]
-__global__ void spline_pass1(const double* __restrict__ in, SplineGrid g, SplineTables tb, double* __restrict__ out)
+__global__ void spline_pass0(const double* __restrict__ W, FieldConst fc, SplineGrid g, SplineTables tb, int q,
+                             double* __restrict__ out)
+{
+    const long long lines = (long long)g.npts * g.npts;
+    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x)
+        pass0_line(W, fc, g, tb, q, out, L);
+}
+
+// pass 1: [M0][N1][N2] along axis 1 -> [M0][M1][N2]; one line (a, k)
+__device__ __forceinline__ void pass1_line(const double* __restrict__ in, const SplineGrid& g, const SplineTables& tb,
+                                           double* __restrict__ out, long long L)
 {
     const int N = g.npts, M = N + g.pad;
-    const long long lines = (long long)M * N;
-    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(L / N), k = (int)(L - (long long)a * N);
-        const double* src = in + (long long)a * N * N + k;
-        auto f = [&](int i) { return src[(long long)i * N]; };
-        line_solve(f, N, g.periodic, tb, out + (long long)a * M * N + k, N);
-    }
+    const int a = (int)(L / N), k = (int)(L - (long long)a * N);
+    const double* src = in + (long long)a * N * N + k;
+    auto f = [&](int i) { return src[(long long)i * N]; };
+    line_solve(f, N, g.periodic, tb, out + (long long)a * M * N + k, N);
+}
+
+__global__ void spline_pass1(const double* __restrict__ in, SplineGrid g, SplineTables tb, double* __restrict__ out)
+{
+    const long long lines = (long long)(g.npts + g.pad) * g.npts;
+    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x)
+        pass1_line(in, g, tb, out, L);
 }
 
 // pass 2: [M0][M1][N2] along axis 2 -> [M0][M1][M2].  Lines are contiguous,
@@ -115,16 +126,14 @@ __global__ void spline_pass1(const double* __restrict__ in, SplineGrid g, Spline
 constexpr int kLineChunk = 32;
 constexpr int kPass2Warps = 4;
 
-__global__ void __launch_bounds__(32 * kPass2Warps) spline_pass2(const double* __restrict__ in, SplineGrid g,
-                                                                 SplineTables tb, double* __restrict__ out)
+// lines [L0, L0 + 32) of a pass-2 input (lines total), by one warp with its staging rows sm
+__device__ __forceinline__ void pass2_group(const double* __restrict__ in, const SplineGrid& g, const SplineTables& tb,
+                                            double* __restrict__ out, long long L0, long long lines,
+                                            double (*sm)[kLineChunk + 1])
 {
-    __shared__ double stage[kPass2Warps][32][kLineChunk + 1];
     const int N = g.npts, M = N + g.pad;
-    const long long lines = (long long)M * M;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double(*sm)[kLineChunk + 1] = stage[warp];
-    const long long nwarps = (long long)gridDim.x * kPass2Warps;
-    for (long long L0 = ((long long)blockIdx.x * kPass2Warps + warp) * 32; L0 < lines; L0 += nwarps * 32) {
+    const int lane = threadIdx.x & 31;
+    {
         const int nl = (int)min(32LL, lines - L0);           // lines of this warp
         const long long myL = L0 + lane;
         const bool mine = lane < nl;
@@ -237,6 +246,18 @@ __global__ void __launch_bounds__(32 * kPass2Warps) spline_pass2(const double* _
     }
 }
 
+__global__ void __launch_bounds__(32 * kPass2Warps) spline_pass2(const double* __restrict__ in, SplineGrid g,
+                                                                 SplineTables tb, double* __restrict__ out)
+{
+    __shared__ double stage[kPass2Warps][32][kLineChunk + 1];
+    const int M = g.npts + g.pad;
+    const long long lines = (long long)M * M;
+    const int warp = threadIdx.x >> 5;
+    const long long nwarps = (long long)gridDim.x * kPass2Warps;
+    for (long long L0 = ((long long)blockIdx.x * kPass2Warps + warp) * 32; L0 < lines; L0 += nwarps * 32)
+        pass2_group(in, g, tb, out, L0, lines, stage[warp]);
+}
+
 struct Basis {
     double w[4];
 };
@@ -322,34 +343,44 @@ __global__ void particles_eval_kernel(Coefs3 cf, SplineGrid g, long long np, con
 // U2 from the new spline at pos + U dt (pos is (y, x, z), U is (u, v, w)),
 // pos += (U + U2) dt / 2, periodic wrap, then U at the new position for the
 // next step's predictor (the reference's getParticleProp at loop start).
+__device__ __forceinline__ void heun_particle(const Coefs3& cf, const SplineGrid& g, double dt, long long p,
+                                              double* __restrict__ py, double* __restrict__ px, double* __restrict__ pz,
+                                              double* __restrict__ Uu, double* __restrict__ Uv, double* __restrict__ Uw)
+{
+    const double twopi = 2.0 * 3.14159265358979311600;   // 2 * atan(1)*4 in double
+    double pos[3] = {py[p], px[p], pz[p]};
+    const double U[3] = {Uu[p], Uv[p], Uw[p]};
+    double U2[3];
+    eval3(cf.c, g, add(pos[0], mul(U[1], dt)), add(pos[1], mul(U[0], dt)), add(pos[2], mul(U[2], dt)), U2);
+    pos[0] = add(pos[0], mul(mul(0.5, add(U[1], U2[1])), dt));
+    pos[1] = add(pos[1], mul(mul(0.5, add(U[0], U2[0])), dt));
+    pos[2] = add(pos[2], mul(mul(0.5, add(U[2], U2[2])), dt));
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        if (pos[q] > twopi) pos[q] = fmod(pos[q], twopi);
+        if (pos[q] < 0) pos[q] = sub(twopi, fmod(-pos[q], twopi));
+    }
+    double Un[3];
+    eval3(cf.c, g, pos[0], pos[1], pos[2], Un);
+    py[p] = pos[0];
+    px[p] = pos[1];
+    pz[p] = pos[2];
+    Uu[p] = Un[0];
+    Uv[p] = Un[1];
+    Uw[p] = Un[2];
+}
+
+// Heun step (src/ParticleTrack.cpp:48-73): U from the previous evaluation,
+// U2 from the new spline at pos + U dt (pos is (y, x, z), U is (u, v, w)),
+// pos += (U + U2) dt / 2, periodic wrap, then U at the new position for the
+// next step's predictor (the reference's getParticleProp at loop start).
 __global__ void particles_heun_kernel(Coefs3 cf, SplineGrid g, const DevClock* __restrict__ clock, long long np,
                                       double* __restrict__ py, double* __restrict__ px, double* __restrict__ pz,
                                       double* __restrict__ Uu, double* __restrict__ Uv, double* __restrict__ Uw)
 {
     const double dt = clock->dt;
-    const double twopi = 2.0 * 3.14159265358979311600;   // 2 * atan(1)*4 in double
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
-        double pos[3] = {py[p], px[p], pz[p]};
-        const double U[3] = {Uu[p], Uv[p], Uw[p]};
-        double U2[3];
-        eval3(cf.c, g, add(pos[0], mul(U[1], dt)), add(pos[1], mul(U[0], dt)), add(pos[2], mul(U[2], dt)), U2);
-        pos[0] = add(pos[0], mul(mul(0.5, add(U[1], U2[1])), dt));
-        pos[1] = add(pos[1], mul(mul(0.5, add(U[0], U2[0])), dt));
-        pos[2] = add(pos[2], mul(mul(0.5, add(U[2], U2[2])), dt));
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            if (pos[q] > twopi) pos[q] = fmod(pos[q], twopi);
-            if (pos[q] < 0) pos[q] = sub(twopi, fmod(-pos[q], twopi));
-        }
-        double Un[3];
-        eval3(cf.c, g, pos[0], pos[1], pos[2], Un);
-        py[p] = pos[0];
-        px[p] = pos[1];
-        pz[p] = pos[2];
-        Uu[p] = Un[0];
-        Uv[p] = Un[1];
-        Uw[p] = Un[2];
-    }
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x)
+        heun_particle(cf, g, dt, p, py, px, pz, Uu, Uv, Uw);
 }
 
 // ---------------------------------------------------------------- stats --
@@ -485,6 +516,62 @@ cudaError_t grid_launch(K kernel, long long work, int threads, cudaStream_t s, A
     return cudaGetLastError();
 }
 
+// ---- ensemble forms: one launch per pass over every member's lines / particles
+__global__ void ensemble_pass0_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm,
+                                      int buf)
+{
+    const long long total = off[nm];
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+        const int m = find_member(off, nm, x);
+        const MemberDev& md = mem[m];
+        const long long local = x - off[m];
+        const long long lines = (long long)md.grid.npts * md.grid.npts;
+        const int q = (int)(local / lines);
+        pass0_line(md.buf[buf], md.fc, md.grid, md.tb, q + 1, md.coef[q], local - q * lines);
+    }
+}
+
+__global__ void ensemble_pass1_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm)
+{
+    const long long total = off[nm];
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+        const int m = find_member(off, nm, x);
+        const MemberDev& md = mem[m];
+        const long long local = x - off[m];
+        const long long lines = (long long)(md.grid.npts + md.grid.pad) * md.grid.npts;
+        const int q = (int)(local / lines);
+        pass1_line(md.coef[q], md.grid, md.tb, md.scratch[q], local - q * lines);
+    }
+}
+
+__global__ void __launch_bounds__(32 * kPass2Warps)
+    ensemble_pass2_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm)
+{
+    __shared__ double stage[kPass2Warps][32][kLineChunk + 1];
+    const int warp = threadIdx.x >> 5;
+    const long long total = off[nm];
+    for (long long w = (long long)blockIdx.x * kPass2Warps + warp; w < total; w += (long long)gridDim.x * kPass2Warps) {
+        const int m = find_member(off, nm, w);
+        const MemberDev& md = mem[m];
+        const long long local = w - off[m];
+        const long long M = md.grid.npts + md.grid.pad;
+        const long long lines = M * M, groups = (lines + 31) / 32;
+        const int q = (int)(local / groups);
+        pass2_group(md.scratch[q], md.grid, md.tb, md.coef[q], (local - q * groups) * 32, lines, stage[warp]);
+    }
+}
+
+__global__ void ensemble_heun_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm)
+{
+    const long long total = off[nm];
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+        const int m = find_member(off, nm, x);
+        const MemberDev& md = mem[m];
+        const Coefs3 cf{{md.coef[0], md.coef[1], md.coef[2]}};
+        heun_particle(cf, md.grid, md.clock->dt, x - off[m], md.P[0], md.P[1], md.P[2], md.P[3], md.P[4], md.P[5]);
+    }
+}
+
 cudaError_t launch_pass2(const double* in, const SplineGrid& g, const SplineTables& tb, double* out, cudaStream_t s)
 {
     const long long M = g.npts + g.pad;
@@ -523,6 +610,26 @@ cudaError_t launch_spline_component(const double* W, const FieldConst& fc, const
     e = grid_launch(spline_pass1, M * N, 128, s, (const double*)coef, g, tb, scratch);
     if (e != cudaSuccess) return e;
     return launch_pass2((const double*)scratch, g, tb, coef, s);
+}
+
+cudaError_t launch_ensemble_splines(const MemberDev* mem, const EnsembleWork& w, const long long totals[3], int nm,
+                                    int buf, cudaStream_t s)
+{
+    cudaError_t e = grid_launch(ensemble_pass0_kernel, totals[0], 128, s, mem, w.line0, nm, buf);
+    if (e != cudaSuccess) return e;
+    e = grid_launch(ensemble_pass1_kernel, totals[1], 128, s, mem, w.line1, nm);
+    if (e != cudaSuccess) return e;
+    long long b = (totals[2] + kPass2Warps - 1) / kPass2Warps;
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    ensemble_pass2_kernel<<<(unsigned)b, 32 * kPass2Warps, 0, s>>>(mem, w.warp2, nm);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ensemble_heun(const MemberDev* mem, const long long* off, int nm, long long total, cudaStream_t s)
+{
+    if (total <= 0) return cudaSuccess;
+    return grid_launch(ensemble_heun_kernel, total, 128, s, mem, off, nm);
 }
 
 cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np, const double* py,

@@ -22,49 +22,16 @@ namespace {
 using sweep_detail::block_max;
 using sweep_detail::wave_speed;
 
-// Periodic ghost refresh: every ghost cell takes the interior cell at the
-// wrapped index (what HaloTransfer produces on a 1x1x1 periodic topology).
 __global__ void halo_kernel(double* __restrict__ W, FieldConst fc, DevClock* clock, int finish_step)
 {
-    const int n = fc.n, nt = fc.nt;
-    const long long nt2 = (long long)nt * nt, nt3 = fc.nt3;
-    const long long r1 = 6 * nt2, r2 = (long long)n * 6 * nt, r3 = (long long)n * n * 6;
-    const long long total = r1 + r2 + r3;
+    const long long total = fc.nt3 - (long long)fc.n * fc.n * fc.n;
     if (finish_step && blockIdx.x == 0 && threadIdx.x == 0) {
         clock->t += clock->dt;   // src/update.cpp:168-169
         clock->iter += 1;
     }
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
-         g += (long long)gridDim.x * blockDim.x) {
-        int j, i, k;
-        if (g < r1) {
-            long long m = g / nt2, rem = g - m * nt2;
-            j = m < 3 ? (int)m : n + (int)m;
-            i = (int)(rem / nt);
-            k = (int)(rem - (long long)i * nt);
-        } else if (g < r1 + r2) {
-            long long h = g - r1;
-            long long per = 6LL * nt;
-            j = 3 + (int)(h / per);
-            long long rem = h - (long long)(j - 3) * per;
-            int m = (int)(rem / nt);
-            i = m < 3 ? m : n + m;
-            k = (int)(rem - (long long)m * nt);
-        } else {
-            long long h = g - r1 - r2;
-            long long per = 6LL * n;
-            j = 3 + (int)(h / per);
-            long long rem = h - (long long)(j - 3) * per;
-            i = 3 + (int)(rem / 6);
-            int m = (int)(rem - (long long)(i - 3) * 6);
-            k = m < 3 ? m : n + m;
-        }
-        auto wrap = [n](int x) { return x < 3 ? x + n : (x >= n + 3 ? x - n : x); };
-        const long long dst = ((long long)j * nt + i) * nt + k;
-        const long long src = ((long long)wrap(j) * nt + wrap(i)) * nt + wrap(k);
-#pragma unroll
-        for (int q = 0; q < 5; q++) W[q * nt3 + dst] = W[q * nt3 + src];
-    }
+         g += (long long)gridDim.x * blockDim.x)
+        halo_cell(W, fc, g);
 }
 
 __global__ void wave_reduce_kernel(const double* __restrict__ W, FieldConst fc, DevClock* clock, int slot)
@@ -163,11 +130,52 @@ cudaError_t set_smem()
 
 }  // namespace
 
+namespace {
+
+// ensemble halo: every member's ghost cells as one flattened index space
+__global__ void ensemble_halo_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm,
+                                     int buf, int finish_step)
+{
+    const long long total = off[nm];
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int m = find_member(off, nm, g);
+        const MemberDev& md = mem[m];
+        const long long local = g - off[m];
+        if (finish_step && local == 0) {
+            md.clock->t += md.clock->dt;
+            md.clock->iter += 1;
+        }
+        halo_cell(md.buf[buf], md.fc, local);
+    }
+}
+
+}  // namespace
+
 cudaError_t sweep_prepare()
 {
     cudaError_t e = set_smem<SweepTile64a>();
     if (e == cudaSuccess) e = set_smem<SweepTile64b>();
+    if (e == cudaSuccess) e = set_ensemble_smem<double, SweepTile64a>();
+    if (e == cudaSuccess) e = set_ensemble_smem<double, SweepTile64b>();
     return e;
+}
+
+cudaError_t launch_ensemble_sweep64(int dir, int variant, const MemberDev* mem, const long long* off, int nm,
+                                    int parity, int seg_len, cudaStream_t s)
+{
+    if (variant == 1) return launch_ensemble_sweep_t<double, SweepTile64b>(dir, mem, off, nm, parity, seg_len, s);
+    return launch_ensemble_sweep_t<double, SweepTile64a>(dir, mem, off, nm, parity, seg_len, s);
+}
+
+cudaError_t launch_ensemble_halo(const MemberDev* mem, const long long* off, int nm, long long total, int buf,
+                                 int finish_step, cudaStream_t s)
+{
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    ensemble_halo_kernel<<<blocks, 256, 0, s>>>(mem, off, nm, buf, finish_step);
+    return cudaGetLastError();
 }
 
 SweepShape sweep_shape(bool mixed, int variant)

@@ -126,14 +126,56 @@ constexpr size_t sweep_smem_bytes()
 
 }  // namespace sweep_detail
 
+// Periodic ghost refresh of ghost cell g (0 <= g < nt^3 - n^3): the ghost
+// takes the interior cell at the wrapped index (what HaloTransfer produces on
+// a 1x1x1 periodic topology).  Ghost cells are enumerated as the 6 ghost
+// y-planes, then the 6 ghost x-rows of the interior y-planes, then the 6
+// ghost z-cells of the interior (y, x) rows.
+__device__ __forceinline__ void halo_cell(double* __restrict__ W, const FieldConst& fc, long long g)
+{
+    const int n = fc.n, nt = fc.nt;
+    const long long nt2 = (long long)nt * nt, nt3 = fc.nt3;
+    const long long r1 = 6 * nt2, r2 = (long long)n * 6 * nt;
+    int j, i, k;
+    if (g < r1) {
+        long long m = g / nt2, rem = g - m * nt2;
+        j = m < 3 ? (int)m : n + (int)m;
+        i = (int)(rem / nt);
+        k = (int)(rem - (long long)i * nt);
+    } else if (g < r1 + r2) {
+        long long h = g - r1;
+        long long per = 6LL * nt;
+        j = 3 + (int)(h / per);
+        long long rem = h - (long long)(j - 3) * per;
+        int m = (int)(rem / nt);
+        i = m < 3 ? m : n + m;
+        k = (int)(rem - (long long)m * nt);
+    } else {
+        long long h = g - r1 - r2;
+        long long per = 6LL * n;
+        j = 3 + (int)(h / per);
+        long long rem = h - (long long)(j - 3) * per;
+        i = 3 + (int)(rem / 6);
+        int m = (int)(rem - (long long)(i - 3) * 6);
+        k = m < 3 ? m : n + m;
+    }
+    auto wrap = [n](int x) { return x < 3 ? x + n : (x >= n + 3 ? x - n : x); };
+    const long long dst = ((long long)j * nt + i) * nt + k;
+    const long long src = ((long long)wrap(j) * nt + wrap(i)) * nt + wrap(k);
+#pragma unroll
+    for (int q = 0; q < 5; q++) W[q * nt3 + dst] = W[q * nt3 + src];
+}
+
+// One CTA's work: the window (bx, by) of faces, segment bz along the normal.
+// Called once per CTA by sweep_kernel and once per work item by the
+// persistent ensemble kernel; every thread of the CTA takes the same path.
 template <int DIR, class T, class Tile>
-__global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepArgs a)
+__device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, int bz, unsigned char* smem_raw)
 {
     using namespace sweep_detail;
     constexpr int kTB = Tile::TB, kTA = Tile::TA, kWB = Tile::WB, kWC = Tile::WC;
     constexpr int kSweepThreads = Tile::threads;
     constexpr bool kMixed = sizeof(T) == 4;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ring = reinterpret_cast<T*>(smem_raw);          // [kRing][kSlabComps][kWC]
     T* rec = ring + kRing * kSlabComps * kWC;          // [10][kWC]
     const FieldConst& fc = a.fc;
@@ -141,8 +183,8 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepA
     const long long nt3 = fc.nt3;
     const Strides st = strides<DIR>(nt);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTB + tx;
-    const int b0 = blockIdx.x * kTB, a0 = blockIdx.y * kTA;
-    const int f_begin = blockIdx.z * a.seg_len;
+    const int b0 = bx * kTB, a0 = by * kTA;
+    const int f_begin = bz * a.seg_len;
     const int f_end = min(f_begin + a.seg_len, n);
     const double dt = step_dt(a);
     // working units: dimensional for double, non-dimensional (dx = 1) for float
@@ -155,7 +197,7 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepA
     const T eps_T = kMixed ? T(fc.eps_T) : T(kWenoEps);
     const double* __restrict__ W = a.W;
 
-    if (DIR == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && tid == 0) {
+    if (DIR == 0 && bx == 0 && by == 0 && bz == 0 && tid == 0) {
         a.clock->wave[a.parity ^ 1] = 0ull;   // the z sweep of this step reduces into it
         a.clock->dt = dt;
     }
@@ -304,6 +346,71 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepA
         if (tid == 0 && m > 0.0) atomicMax(&a.clock->wave[a.parity ^ 1], (unsigned long long)__double_as_longlong(m));
         if (bad) atomicOr(&a.clock->status, 1);
     }
+}
+
+template <int DIR, class T, class Tile>
+__global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    sweep_block<DIR, T, Tile>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
+// Persistent form for an ensemble: a fixed grid of CTAs walks the flattened
+// (member, window, segment) work list of one sweep direction.  Every member
+// uses segments of seg_len faces; off[] are the members' work-item offsets.
+template <int DIR, class T, class Tile>
+__global__ void __launch_bounds__(Tile::threads, Tile::ctas)
+    ensemble_sweep_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm, int parity,
+                          int seg_len)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const long long total = off[nm];
+    for (long long item = blockIdx.x; item < total; item += gridDim.x) {
+        const int m = find_member(off, nm, item);
+        const MemberDev& md = mem[m];
+        const long long local = item - off[m];
+        const int nseg = md.nseg[DIR];
+        const int tb = md.tiles_b[DIR];
+        const int bz = (int)(local % nseg);
+        const long long t = local / nseg;
+        SweepArgs a;
+        a.W = md.buf[parity];
+        a.A = md.buf[parity ^ 1];
+        a.fc = md.fc;
+        a.clock = md.clock;
+        a.parity = parity;
+        a.dt_fixed_mode = md.dt_fixed_mode;
+        a.dt_fixed = md.dt_fixed;
+        a.seg_len = seg_len;
+        sweep_block<DIR, T, Tile>(a, (int)(t % tb), (int)(t / tb), bz, smem_raw);
+        __syncthreads();   // the next item reuses the shared-memory ring
+    }
+}
+
+template <class T, class Tile>
+cudaError_t launch_ensemble_sweep_t(int dir, const MemberDev* mem, const long long* off, int nm, int parity,
+                                    int seg_len, cudaStream_t s)
+{
+    const size_t smem = sweep_detail::sweep_smem_bytes<T, Tile>();
+    const dim3 block(Tile::TB, Tile::TA);
+    const int grid = 148 * Tile::ctas;
+    if (dir == 0) ensemble_sweep_kernel<0, T, Tile><<<grid, block, smem, s>>>(mem, off, nm, parity, seg_len);
+    else if (dir == 1) ensemble_sweep_kernel<1, T, Tile><<<grid, block, smem, s>>>(mem, off, nm, parity, seg_len);
+    else ensemble_sweep_kernel<2, T, Tile><<<grid, block, smem, s>>>(mem, off, nm, parity, seg_len);
+    return cudaGetLastError();
+}
+
+template <class T, class Tile>
+cudaError_t set_ensemble_smem()
+{
+    const int bytes = (int)sweep_detail::sweep_smem_bytes<T, Tile>();
+    cudaError_t e = cudaFuncSetAttribute(ensemble_sweep_kernel<0, T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ensemble_sweep_kernel<1, T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ensemble_sweep_kernel<2, T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
 }
 
 }  // namespace gkm

@@ -36,7 +36,15 @@ cudaError_t sweep_mixed_prepare()
         e = cudaFuncSetAttribute(sweep_kernel<1, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(sweep_kernel<2, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = set_ensemble_smem<float, Tile>();
     return e;
+}
+
+cudaError_t launch_ensemble_sweep32(int dir, int variant, const MemberDev* mem, const long long* off, int nm,
+                                    int parity, int seg_len, cudaStream_t s)
+{
+    (void)variant;
+    return launch_ensemble_sweep_t<float, SweepTile32a>(dir, mem, off, nm, parity, seg_len, s);
 }
 
 cudaError_t launch_sweep_mixed(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s)

@@ -47,25 +47,38 @@ def _w5(W: np.ndarray):
     return (_dp * 5)(*[_ptr(W[q]) for q in range(5)])
 
 
+def make_config(params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
+                max_particles: int = 0, device: int = 0, use_graphs: bool = True,
+                precision: int = 0) -> _capi.GkmConfig:
+    L = _capi.lib()
+    cfg = _capi.GkmConfig()
+    L.gkm_config_default(C.byref(cfg))
+    cfg.params = _capi.GkmParams(n=params.n, gam=params.gam, den0=params.den0, Mt=params.Mt, Re=params.Re,
+                                 mu0=params.mu0, p0=params.p0, t0=params.t0)
+    cfg.cfl = cfl
+    cfg.visc_law = visc_law
+    cfg.spline_mode = spline_mode
+    cfg.device = device
+    cfg.max_particles = max_particles
+    cfg.use_graphs = 1 if use_graphs else 0
+    cfg.precision = precision   # 0 FP64, 1 mixed (FP32 reconstruction + flux, FP64 state)
+    return cfg
+
+
 class Solver:
     def __init__(self, params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
-                 max_particles: int = 0, device: int = 0, use_graphs: bool = True, precision: int = 0):
+                 max_particles: int = 0, device: int = 0, use_graphs: bool = True, precision: int = 0,
+                 _member_handle=None):
         self.L = _capi.lib()
-        cfg = _capi.GkmConfig()
-        self.L.gkm_config_default(C.byref(cfg))
-        cfg.params = _capi.GkmParams(n=params.n, gam=params.gam, den0=params.den0, Mt=params.Mt, Re=params.Re,
-                                     mu0=params.mu0, p0=params.p0, t0=params.t0)
-        cfg.cfl = cfl
-        cfg.visc_law = visc_law
-        cfg.spline_mode = spline_mode
-        cfg.device = device
-        cfg.max_particles = max_particles
-        cfg.use_graphs = 1 if use_graphs else 0
-        cfg.precision = precision   # 0 FP64, 1 mixed (FP32 reconstruction + flux, FP64 state)
-        h = C.c_void_p()
-        s = self.L.gkm_create(C.byref(cfg), C.byref(h))
-        if s != 0:
-            raise GkmError(s, "gkm_create failed (see stderr)")
+        self._owned = _member_handle is None
+        if self._owned:
+            cfg = make_config(params, cfl, visc_law, spline_mode, max_particles, device, use_graphs, precision)
+            h = C.c_void_p()
+            s = self.L.gkm_create(C.byref(cfg), C.byref(h))
+            if s != 0:
+                raise GkmError(s, "gkm_create failed (see stderr)")
+        else:
+            h = C.c_void_p(_member_handle)
         self.h = h
         self.params = params
         self.n = params.n
@@ -80,7 +93,8 @@ class Solver:
 
     def close(self) -> None:
         if getattr(self, "h", None):
-            self.L.gkm_destroy(self.h)
+            if self._owned:
+                self.L.gkm_destroy(self.h)
             self.h = None
 
     def __enter__(self):
@@ -188,6 +202,93 @@ class Solver:
         st = _capi.GkmStats()
         self._check(self.L.gkm_stats_compute(self.h, C.byref(st)))
         return st.as_dict()
+
+
+class Ensemble:
+    """Many independent cubes stepped together, one launch per stage (gkm_ensemble_*).
+
+    ``members`` is a list of dicts with the keyword arguments of Solver
+    (params, cfl, visc_law, spline_mode, max_particles); all share ``device``
+    and ``precision``.  ``ens[m]`` is a Solver view of member m (upload_state,
+    download_state, particles_upload, print_stats, clock, ... act on that
+    member); the ensemble owns the members.
+    """
+
+    def __init__(self, members: list, device: int = 0, precision: int = 0):
+        self.L = _capi.lib()
+        cfgs = (_capi.GkmConfig * len(members))()
+        for i, m in enumerate(members):
+            cfgs[i] = make_config(m["params"], m.get("cfl", 0.10), m.get("visc_law", 0), m.get("spline_mode", 0),
+                                  m.get("max_particles", 0), device, True, precision)
+        h = C.c_void_p()
+        s = self.L.gkm_ensemble_create(cfgs, len(members), C.byref(h))
+        if s != 0:
+            raise GkmError(s, "gkm_ensemble_create failed (see stderr)")
+        self.h = h
+        self.members = [Solver(m["params"], spline_mode=m.get("spline_mode", 0),
+                               _member_handle=self.L.gkm_ensemble_member(h, i)) for i, m in enumerate(members)]
+
+    def _check(self, s: int) -> None:
+        if s != 0:
+            raise GkmError(s, self.L.gkm_ensemble_last_error(self.h).decode())
+
+    def __len__(self) -> int:
+        return len(self.members)
+
+    def __getitem__(self, m: int) -> Solver:
+        return self.members[m]
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            for m in self.members:
+                m.h = None
+            self.L.gkm_ensemble_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, nsteps: int = 1, with_particles: bool = True) -> None:
+        self._check(self.L.gkm_ensemble_step(self.h, nsteps, 1 if with_particles else 0))
+
+    def step_timed(self, nsteps: int, with_particles: bool = True) -> dict:
+        ms = np.zeros(7)
+        self._check(self.L.gkm_ensemble_step_timed(self.h, nsteps, 1 if with_particles else 0, _ptr(ms)))
+        keys = ("sweep_x", "sweep_y", "sweep_z", "halo", "splines", "particles", "total")
+        return dict(zip(keys, ms.tolist()))
+
+    def autotune(self, reps: int = 2) -> list:
+        self._check(self.L.gkm_ensemble_autotune(self.h, reps))
+        return self.sweep_config()
+
+    def sweep_config(self) -> list:
+        out = (C.c_int32 * 12)()
+        self._check(self.L.gkm_ensemble_sweep_config(self.h, out))
+        return [{"dir": "xyz"[d], "variant": out[4 * d], "window": [out[4 * d + 1], out[4 * d + 2]],
+                 "segment": out[4 * d + 3]} for d in range(3)]
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._check(self.L.gkm_ensemble_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def synchronize(self) -> None:
+        self._check(self.L.gkm_ensemble_synchronize(self.h))
+
+    def stream(self) -> int:
+        """The ensemble's cudaStream_t as an integer (torch.cuda.ExternalStream accepts it)."""
+        p = C.c_void_p()
+        self._check(self.L.gkm_ensemble_stream(self.h, C.byref(p)))
+        return p.value or 0
 
 
 def probe_fma_peak(device: int = 0):

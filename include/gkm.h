@@ -235,6 +235,51 @@ gkm_status gkm_set_stream(gkm_handle* h, void* stream);
  * valid until the next step. */
 gkm_status gkm_device_state(gkm_handle* h, double** W);
 
+/* ---------------------------------------------------------------- ensemble
+ *
+ * Many independent periodic cubes (grid size, Mt, Re, seed, particles may all
+ * differ) stepped together on one GPU.  No reference counterpart: the
+ * reference runs one cube per job (src/Main.cpp:10-49), and a parameter
+ * sweep there is one job per case.  Each stage of a step is ONE launch over a
+ * flattened work list of every member: the x, y, z sweeps (persistent CTAs
+ * walking (member, window, segment) items), the ghost wrap, the three spline
+ * passes and the Heun advection.  A step is captured as one CUDA graph per
+ * buffer parity.  Every member evolves exactly as the same cube stepped alone
+ * through gkm_step (bit for bit with the same sweep segment length).
+ *
+ * All members share the device, the precision and the ensemble's stream.
+ * gkm_ensemble_member returns a member's handle for the single-cube calls
+ * (gkm_upload_state, gkm_download_state, gkm_particles_upload/download,
+ * gkm_stats_compute, gkm_get_clock, gkm_set_dt, ...); those calls run on the
+ * ensemble's stream.  gkm_destroy and gkm_set_stream refuse member handles.
+ * gkm_ensemble_step needs every member's state uploaded and all members at
+ * the same buffer parity (true when they were uploaded and then stepped only
+ * by the ensemble). */
+typedef struct gkm_ensemble gkm_ensemble;
+
+gkm_status gkm_ensemble_create(const gkm_config* members, int32_t n_members, gkm_ensemble** out);
+gkm_status gkm_ensemble_destroy(gkm_ensemble* e);
+const char* gkm_ensemble_last_error(const gkm_ensemble* e);
+int32_t gkm_ensemble_size(const gkm_ensemble* e);
+gkm_handle* gkm_ensemble_member(gkm_ensemble* e, int32_t m);
+/* nsteps full steps (Eulerian + ghost wrap, and with with_particles the
+ * splines of the new state and Heun advection of every member's particles). */
+gkm_status gkm_ensemble_step(gkm_ensemble* e, int32_t nsteps, int32_t with_particles);
+/* As gkm_ensemble_step without graphs, with CUDA-event times summed over the
+ * steps: ms[0..2] x/y/z sweeps, ms[3] ghost wrap, ms[4] splines,
+ * ms[5] particles, ms[6] whole steps. */
+gkm_status gkm_ensemble_step_timed(gkm_ensemble* e, int32_t nsteps, int32_t with_particles, double ms[7]);
+/* Times every window variant x segment length of each sweep direction over
+ * the whole ensemble (reps launches each) and keeps the fastest; the state is
+ * untouched and every member's clock is restored. */
+gkm_status gkm_ensemble_autotune(gkm_ensemble* e, int32_t reps);
+/* out[4d..4d+3] = window variant, window width, window height, segment length */
+gkm_status gkm_ensemble_sweep_config(const gkm_ensemble* e, int32_t out[12]);
+gkm_status gkm_ensemble_launch_count(const gkm_ensemble* e, int64_t* count);
+gkm_status gkm_ensemble_synchronize(gkm_ensemble* e);
+/* The ensemble's stream (cudaStream_t as void*), for events or interop. */
+gkm_status gkm_ensemble_stream(const gkm_ensemble* e, void** stream);
+
 #ifdef __cplusplus
 }
 #endif
