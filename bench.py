@@ -65,11 +65,22 @@ def cells_of(n: int) -> int:
     return n ** 3
 
 
-def workload(n=N_CELLS, npart=N_PART):
-    return {"workload": f"{n}^3 periodic cube, FP64 drop-in, Mt {MT}, Re_lambda {RE:g}, {npart} particles, "
+# (Mt, Re_lambda) per cube size: 64^3 and 256^3 as the 64^3 / 256^3 cases, 512^3 and 1024^3 the large ones
+SIZES = {64: (0.3, 30.0), 256: (MT, RE), 512: (0.5, 100.0), 1024: (0.4, 150.0)}
+
+
+def case_of(n: int):
+    return SIZES.get(n, (MT, RE))
+
+
+def workload(n=N_CELLS, npart=N_PART, precision="fp64"):
+    Mt, Re = case_of(n)
+    form = "FP64 drop-in" if precision == "fp64" else "mixed precision (FP32 WENO + flux, FP64 state)"
+    nt = n + 6
+    return {"workload": f"{n}^3 periodic cube, {form}, Mt {Mt}, Re_lambda {Re:g}, {npart} particles, "
                         f"cfl {CFL}, natural_ghost3 splines",
-            "n": n, "particles": npart, "cfl": CFL, "precision": "fp64", "seed": SEED,
-            "l2": "no flush: resident state 2 x 1.44 GB and splines 0.44 GB exceed the 126 MB L2",
+            "n": n, "particles": npart, "cfl": CFL, "precision": precision, "seed": SEED,
+            "l2": f"no flush: resident state 2 x {5 * nt ** 3 * 8 / 1e9:.2f} GB exceeds the 126 MB L2",
             "parallelism": "replicas"}
 
 
@@ -279,18 +290,25 @@ def ours(args, rank: int, world: int, local_rank: int):
     if dist:
         import torch.distributed as tdist
     n, npart = args.n, args.particles
-    P, u, v, w, rho, p = ic.make_field(n, MT, RE, SEED + rank)
-    W0 = ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, p))
-    del u, v, w, rho, p
+    Mt, Re = case_of(n)
+    prec = 1 if args.precision == "mixed" else 0
+    if n > 256:
+        # cuFFT-based restatement of the recipe: the NumPy one needs tens of GB of host memory here
+        P, W0 = ic.make_state_device(n, Mt, Re, SEED + rank, device=f"cuda:{local_rank}")
+        torch.cuda.empty_cache()
+    else:
+        P, u, v, w, rho, p = ic.make_field(n, Mt, Re, SEED + rank)
+        W0 = ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, p))
+        del u, v, w, rho, p
     pos0 = ic.particles_to_reference_order(ic.make_particles(npart, SEED + rank))
 
     fp64_peak, fp32_peak = probe_fma_peak(local_rank)
     stream = torch.cuda.Stream()
-    s = Solver(P, cfl=CFL, max_particles=npart, device=local_rank)
+    s = Solver(P, cfl=CFL, max_particles=npart, device=local_rank, precision=prec)
     s.set_stream(stream.cuda_stream)
     s.upload_state(W0)
     s.particles_upload(pos0)
-    sweep_cfg = s.autotune(2)
+    sweep_cfg = s.autotune(args.autotune_reps)
     s.step_timed(args.warmup, True)
     torch.cuda.synchronize()
 
@@ -315,18 +333,51 @@ def ours(args, rank: int, world: int, local_rank: int):
         t = torch.tensor([eul_ms, part_ms, total_ms], dtype=torch.float64, device="cuda")
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         eul_ms, part_ms, total_ms = t.tolist()
-
-    # the mixed-precision form on the same input and step count; error against this FP64 run
     nt = s.nt
-    forms = {}
-    if not args.no_forms:
+    state_bytes = 5 * nt ** 3 * 8
+    do_forms = not args.no_forms and prec == 0
+    if do_forms:   # FP64 state after warmup + steps, the reference point of the mixed form
         W64 = s.download_state()
         tke64 = s.print_stats()["TKE"]
+
+    # end to end through the plug point evolve(W, dt): pinned host W in, one step, W out
+    e2e = None
+    if not args.no_e2e:
+        Wh = torch.empty((5, nt, nt, nt), dtype=torch.float64, pin_memory=True)
+        Wn = Wh.numpy()
+        s.download_state(Wn)
+        dt = s.timestep()
+        s.evolve(Wn, dt)   # warm-up of the copy path
+        torch.cuda.synchronize()
+        if dist:
+            tdist.barrier()
+        x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        x0.record(stream)
+        for _ in range(args.steps):
+            s.evolve(Wn, dt)
+        x1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = x0.elapsed_time(x1)
+        if dist:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+            e2e_ms = t.item()
+            tdist.barrier()
+        del Wh, Wn
+        e2e = {"value": world * n ** 3 * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+               "api": "gkm_evolve(h, W, dt): the reference's evolve(W, dev, dt) plug point"}
+    clocks = sampler.stop()
+
+    # the mixed-precision form on the same input and step count; error against the FP64 run
+    forms = {}
+    s.close()
+    if do_forms:
         m = Solver(P, cfl=CFL, max_particles=npart, device=local_rank, precision=1)
         m.set_stream(stream.cuda_stream)
         m.upload_state(W0)
         m.particles_upload(pos0)
-        m_cfg = m.autotune(2)
+        m_cfg = m.autotune(args.autotune_reps)
         m.step_timed(args.warmup, True)
         mph = m.step_timed(args.steps, True)
         Wm = m.download_state()
@@ -336,38 +387,16 @@ def ours(args, rank: int, world: int, local_rank: int):
         err = [float(np.linalg.norm(Wm[q, sl, sl, sl] - W64[q, sl, sl, sl]) / np.linalg.norm(W64[q, sl, sl, sl]))
                for q in range(5)]
         m_eul = mph["sweep_x"] + mph["sweep_y"] + mph["sweep_z"] + mph["halo"]
-        forms["mixed"] = {"value": world * cells_of(n) * args.steps / (m_eul * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+        forms["mixed"] = {"value": world * n ** 3 * args.steps / (m_eul * 1e-3) / 1e9, "unit": "Gcell-updates/s",
                           "particle_steps_per_s": world * npart * args.steps / ((mph["splines"] + mph["particles"]) * 1e-3),
                           "ms_per_step": mph["total"] / args.steps,
+                          "phases_ms_per_step": {k: v / args.steps for k, v in mph.items()},
                           "rel_l2_vs_fp64": dict(zip(("rho", "rho_u", "rho_v", "rho_w", "rho_E"), err)),
                           "tke_rel_err_vs_fp64": abs(tkem - tke64) / tke64,
                           "steps_compared": args.warmup + args.steps, "sweep_shapes": m_cfg}
         del W64, Wm
-        forms.update(batched_forms(args, local_rank, stream))
-
-    # end to end through the plug point evolve(W, dt): pinned host W in, one step, W out
-    Wh = torch.empty((5, nt, nt, nt), dtype=torch.float64, pin_memory=True)
-    Wn = Wh.numpy()
-    s.download_state(Wn)
-    dt = s.timestep()
-    s.evolve(Wn, dt)   # warm-up of the copy path
-    torch.cuda.synchronize()
-    if dist:
-        tdist.barrier()
-    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    x0.record(stream)
-    for _ in range(args.steps):
-        s.evolve(Wn, dt)
-    x1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = x0.elapsed_time(x1)
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e_ms = t.item()
-        tdist.barrier()
-    clocks = sampler.stop()
-    s.close()
+        if not args.no_batched:
+            forms.update(batched_forms(args, local_rank, stream))
     if rank != 0:
         return
 
@@ -381,26 +410,24 @@ def ours(args, rank: int, world: int, local_rank: int):
     achieved = flops_launch / launch_s / 1e12
     bytes_launch = (80 + 120 + 120) / 3 * cells             # compulsory W read + accumulator traffic
     traffic = None if SWEEP_DRAM_BYTES_PER_CELL is None else SWEEP_DRAM_BYTES_PER_CELL * cells
-    state_bytes = 5 * nt ** 3 * 8
+    peak = fp32_peak if prec else fp64_peak
 
     line = {"metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec else "f64",
             "data": "synthetic: seeded solenoidal field (init_DNS recipe), uniform particles",
-            "config": workload(n, npart),
+            "config": workload(n, npart, args.precision),
             "particle_steps_per_s": world * npart * args.steps / (part_ms * 1e-3),
             "phases_ms_per_step": {k: v / args.steps for k, v in ph.items()},
-            "roofline": {"kernel": "sweep_kernel (x/y/z, one launch each per step)", "bound": "fp64",
-                         "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
-                         "traffic": traffic, "flops_per_cell_update": flops_cell,
-                         "peak_source": "FP64 FMA probe run by this bench (gkm_probe_fma_peak)",
+            "roofline": {"kernel": "sweep_kernel (x/y/z, one launch each per step)", "bound": "fp32" if prec else "fp64",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": traffic if not prec else None, "flops_per_cell_update": flops_cell,
+                         "peak_source": "FMA probe run by this bench (gkm_probe_fma_peak)",
                          "hbm": {"achieved_gbs": bytes_launch / launch_s / 1e9, "peak_gbs": HBM_PEAK_GBS,
                                  "frac": bytes_launch / launch_s / 1e9 / HBM_PEAK_GBS,
                                  "peak_source": "measured copy bandwidth"}},
             "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
-            "e2e": {"value": world * cells * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
-                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
-                    "api": "gkm_evolve(h, W, dt): the reference's evolve(W, dev, dt) plug point"},
+            "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, "sweep_shapes": sweep_cfg, "forms": forms}
     if world == 1 and not args.no_cpu_baseline:
         workers = max(1, min(os.cpu_count() or 1, 8))
@@ -423,6 +450,10 @@ def main():
     ap.add_argument("--particles", type=int, default=N_PART)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed-precision and batched forms")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched ensemble forms")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer plug-point measurement")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="form of the main line")
+    ap.add_argument("--autotune-reps", type=int, default=2, help="timed launches per sweep shape")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -28,7 +28,15 @@ EXPORTS = [
     "gkm_ensemble_create", "gkm_ensemble_destroy", "gkm_ensemble_last_error", "gkm_ensemble_size",
     "gkm_ensemble_member", "gkm_ensemble_step", "gkm_ensemble_step_timed", "gkm_ensemble_autotune",
     "gkm_ensemble_sweep_config", "gkm_ensemble_launch_count", "gkm_ensemble_synchronize", "gkm_ensemble_stream",
+    "gkm_particle_props", "gkm_particle_stats_compute", "gkm_write_field", "gkm_write_particles", "gkm_write_time",
+    "gkm_write_reinit",
 ]
+
+PROP_COUNT = 41
+PROP_NAMES = (["rho"] + [f"grad_rho_{a}" for a in "yxz"] + ["u", "v", "w"]
+              + [f"grad_{c}_{a}" for c in "uvw" for a in "yxz"] + ["p"] + [f"grad_p_{a}" for a in "yxz"]
+              + [f"hess_p_{a}{b}" for a in "yxz" for b in "yxz"] + ["lap_u", "lap_v", "lap_w"]
+              + [f"grad_lap_{c}_{a}" for c in "uvw" for a in "yxz"])
 
 
 class GkmParams(C.Structure):
@@ -41,6 +49,14 @@ class GkmConfig(C.Structure):
     _fields_ = [("params", GkmParams), ("cfl", C.c_double), ("visc_law", C.c_int32), ("spline_mode", C.c_int32),
                 ("precision", C.c_int32), ("device", C.c_int32), ("max_particles", C.c_int64),
                 ("use_graphs", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+class GkmParticleStats(C.Structure):
+    _fields_ = [("TKE", C.c_double), ("SijSij", C.c_double), ("SKEWu", C.c_double), ("SKEWw", C.c_double),
+                ("count", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class GkmStats(C.Structure):
@@ -107,6 +123,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.gkm_ensemble_launch_count.argtypes = [_h, C.POINTER(C.c_int64)]
     L.gkm_ensemble_synchronize.argtypes = [_h]
     L.gkm_ensemble_stream.argtypes = [_h, C.POINTER(C.c_void_p)]
+    L.gkm_particle_props.argtypes = [_h, _dp]
+    L.gkm_particle_stats_compute.argtypes = [_h, C.POINTER(GkmParticleStats)]
+    for w in ("gkm_write_field", "gkm_write_particles", "gkm_write_time", "gkm_write_reinit"):
+        getattr(L, w).argtypes = [_h, C.c_char_p]
     for name in EXPORTS:
         if name not in ("gkm_config_default", "gkm_last_error", "gkm_ensemble_last_error", "gkm_ensemble_member"):
             getattr(L, name).restype = st   # gkm_status, or int for gkm_abi_version / gkm_nt

@@ -20,7 +20,7 @@ LIBDIR = os.path.join(PKG, "lib")
 OBJDIR = os.path.join(PKG, "lib", "obj")
 LIB = os.path.join(LIBDIR, "libgkm_b200.so")
 
-SOURCES = ["sweep.cu", "sweep_mixed.cu", "lagrangian.cu", "probe.cu", "noalloc.cu", "gkm_capi.cu", "gkm_ensemble.cu"]
+SOURCES = ["sweep.cu", "sweep_mixed.cu", "lagrangian.cu", "probe.cu", "noalloc.cu", "gkm_capi.cu", "gkm_ensemble.cu", "output.cu"]
 HEADERS = ["gkm_numerics.cuh", "gkm_internal.h", "gkm_handle.h", "sweep_impl.cuh"]
 # per-file extra flags: the single-precision sweeps use fast float math
 EXTRA = {"sweep_mixed.cu": ["-use_fast_math", "-DGKM_UNROLL_SIDES=0"]}

@@ -132,7 +132,8 @@ cudaError_t enqueue_eulerian(gkm_handle* h)
         if (e != cudaSuccess) return e;
     }
     h->launches += 4;
-    return gkm::launch_halo(h->buf[h->parity ^ 1], h->fc, h->clock, 1, h->stream);
+    return gkm::launch_halo(h->buf[h->parity ^ 1], h->fc, h->clock, 1, h->parity ^ 1, h->dt_fixed_mode, h->dt_fixed,
+                            h->stream);
 }
 
 cudaError_t enqueue_splines(gkm_handle* h, const double* W)
@@ -231,7 +232,54 @@ gkm_status ensure_splines(gkm_handle* h)
     return GKM_OK;
 }
 
+// the five further splines of the reference's 8-field generateSplines
+// (src/update.cpp:1200-1233) and getParticleProp for every particle
+// (src/ParticleTrack.cpp:99-113) into h->props; allocates on first use
+gkm_status compute_props(gkm_handle* h)
+{
+    gkm_status s = ensure_splines(h);
+    if (s != GKM_OK) return s;
+    const long long M = h->grid.npts + h->grid.pad;
+    for (int c = 0; c < 5; c++)
+        if (!h->prop_coef[c]) CK(h, cudaMalloc(&h->prop_coef[c], sizeof(double) * (size_t)(M * M * M)));
+    if (!h->lap_nodes) CK(h, cudaMalloc(&h->lap_nodes, sizeof(double) * (size_t)h->fc.nt3));
+    if (!h->props && h->cap > 0) CK(h, cudaMalloc(&h->props, sizeof(double) * gkm::kPropCount * (size_t)h->cap));
+    const gkm::SplineTables tb = device_tables(h);
+    const double* W = h->buf[h->parity];
+    CK(h, gkm::launch_spline_source(W, h->fc, h->grid, tb, gkm::kSplineDensity, h->prop_coef[0], h->scratch,
+                                    h->stream));
+    CK(h, gkm::launch_spline_source(W, h->fc, h->grid, tb, gkm::kSplinePressure, h->prop_coef[1], h->scratch,
+                                    h->stream));
+    for (int f = 0; f < 3; f++) {
+        CK(h, gkm::launch_lap_nodes(h->coef[f], h->grid, h->fc, h->lap_nodes, h->stream));
+        CK(h, gkm::launch_spline_source(h->lap_nodes, h->fc, h->grid, tb, gkm::kSplinePlain, h->prop_coef[2 + f],
+                                        h->scratch, h->stream));
+    }
+    h->launches += 2 * 3 + 3 * (1 + 3);
+    if (h->np > 0) {
+        const double* c8[8] = {h->prop_coef[0], h->coef[0], h->coef[1], h->coef[2],
+                               h->prop_coef[1], h->prop_coef[2], h->prop_coef[3], h->prop_coef[4]};
+        CK(h, gkm::launch_particle_props(c8, h->grid, h->np, h->P[0], h->P[1], h->P[2], h->props, h->stream));
+        h->launches += 1;
+    }
+    return GKM_OK;
+}
+
 }  // namespace
+
+// host copy of the property table, particle-major (np x kPropCount); used by the writers too
+gkm_status gkm_host_props(gkm_handle* h, double* out)
+{
+    gkm_status s = compute_props(h);
+    if (s != GKM_OK || h->np == 0) return s;
+    std::vector<double> tmp((size_t)gkm::kPropCount * (size_t)h->np);
+    CK(h, cudaMemcpyAsync(tmp.data(), h->props, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const size_t np = (size_t)h->np;
+    for (size_t p = 0; p < np; p++)
+        for (int q = 0; q < gkm::kPropCount; q++) out[p * gkm::kPropCount + q] = tmp[(size_t)q * np + p];
+    return GKM_OK;
+}
 
 extern "C" {
 
@@ -382,6 +430,9 @@ gkm_status gkm_destroy(gkm_handle* h)
     for (int c = 0; c < 3; c++) cudaFree(h->coef[c]);
     cudaFree(h->scratch);
     for (int c = 0; c < 6; c++) cudaFree(h->P[c]);
+    for (int c = 0; c < 5; c++) cudaFree(h->prop_coef[c]);
+    cudaFree(h->lap_nodes);
+    cudaFree(h->props);
     cudaFree(h->partials);
     cudaFree(h->stats_out);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -397,9 +448,9 @@ gkm_status gkm_upload_state(gkm_handle* h, const double* const W[5])
     const size_t bytes = sizeof(double) * (size_t)h->fc.nt3;
     double* dst = h->buf[h->parity];
     for (int q = 0; q < 5; q++)
-        CK(h, cudaMemcpyAsync(dst + (size_t)q * h->fc.nt3, W[q], bytes, cudaMemcpyHostToDevice, h->stream));
+        CK(h, cudaMemcpyAsync(dst + (size_t)q * h->fc.nt3, W[q], bytes, cudaMemcpyDefault, h->stream));
     h->launches += 1;
-    CK(h, gkm::launch_halo(dst, h->fc, h->clock, 0, h->stream));
+    CK(h, gkm::launch_halo(dst, h->fc, h->clock, 0, h->parity, 0, 0.0, h->stream));
     CK(h, cudaMemsetAsync(&h->clock->status, 0, sizeof(int), h->stream));
     gkm_status s = reduce_wave(h);
     if (s != GKM_OK) return s;
@@ -416,7 +467,7 @@ gkm_status gkm_download_state(gkm_handle* h, double* const W[5])
     const double* src = h->buf[h->parity];
     for (int q = 0; q < 5; q++) {
         if (!W[q]) return fail(h, GKM_ERR_ARG, "W[q] is NULL");
-        CK(h, cudaMemcpyAsync(W[q], src + (size_t)q * h->fc.nt3, bytes, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaMemcpyAsync(W[q], src + (size_t)q * h->fc.nt3, bytes, cudaMemcpyDefault, h->stream));
     }
     DevClock c;
     return read_clock(h, &c);
@@ -478,7 +529,9 @@ gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles,
             e = launch_sweep_any(h, d, a);
             if (e == cudaSuccess) e = cudaEventRecord(ev[d + 1], h->stream);
         }
-        if (e == cudaSuccess) e = gkm::launch_halo(h->buf[h->parity ^ 1], h->fc, h->clock, 1, h->stream);
+        if (e == cudaSuccess)
+            e = gkm::launch_halo(h->buf[h->parity ^ 1], h->fc, h->clock, 1, h->parity ^ 1, h->dt_fixed_mode,
+                                 h->dt_fixed, h->stream);
         if (e == cudaSuccess) e = cudaEventRecord(ev[4], h->stream);
         h->launches += 4;
         h->parity ^= 1;
@@ -730,6 +783,36 @@ gkm_status gkm_stats_compute(gkm_handle* h, gkm_stats* out)
     out->Prms = v[16] / (gam * P.p0 * Mt * Mt);
     out->Trms = v[17] / ((gam - 1) * h->fc.T0 * Mt * Mt);
     out->Vrms = v[18] / (Mt * Mt / P.den0);
+    return GKM_OK;
+}
+
+gkm_status gkm_particle_props(gkm_handle* h, double* props)
+{
+    if (!h || (h->np > 0 && !props)) return GKM_ERR_ARG;
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    return gkm_host_props(h, props);
+}
+
+gkm_status gkm_particle_stats_compute(gkm_handle* h, gkm_particle_stats* out)
+{
+    if (!h || !out) return GKM_ERR_ARG;
+    if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "no state uploaded");
+    if (h->np <= 0) return fail(h, GKM_ERR_STATE, "no particles uploaded");
+    gkm_status s = compute_props(h);
+    if (s != GKM_OK) return s;
+    h->launches += 2;
+    CK(h, gkm::launch_particle_stats(h->props, h->np, h->partials, kStatsBlocks, h->stats_out, h->stream));
+    double v[6];
+    CK(h, cudaMemcpyAsync(v, h->stats_out, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    // src/update.cpp:1148-1155
+    const double n = (double)h->np;
+    out->TKE = v[0] / n;
+    out->SijSij = v[1] / n;
+    const double dudx2 = v[2] / n, dudx3 = v[3] / n, dwdz2 = v[4] / n, dwdz3 = v[5] / n;
+    out->SKEWu = dudx3 / std::pow(dudx2, 1.5);
+    out->SKEWw = dwdz3 / std::pow(dwdz2, 1.5);
+    out->count = h->np;
     return GKM_OK;
 }
 

@@ -34,6 +34,9 @@ struct gkm_handle {
     bool splines_valid = false;
     int64_t np = 0, cap = 0;
     double* P[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // y, x, z, u, v, w
+    double* prop_coef[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // rho, p, lap u, lap v, lap w
+    double* lap_nodes = nullptr;     // nt^3 Laplacian node values (one velocity component at a time)
+    double* props = nullptr;         // [kPropCount][cap] particle properties
     gkm::StatsPartial* partials = nullptr;
     double* stats_out = nullptr;
     cudaGraphExec_t graph[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
@@ -43,6 +46,9 @@ struct gkm_handle {
     std::string err;
     gkm_ensemble* owner = nullptr;   // set while the handle is a member of an ensemble
 };
+
+// particle property table on the host, particle-major np x kPropCount (gkm_capi.cu)
+gkm_status gkm_host_props(gkm_handle* h, double* out);
 
 namespace gkm_host {
 

@@ -12,7 +12,9 @@ namespace gkm {
 // step never waits for the host.
 struct DevClock {
     double dt;                   // dt of the step being taken (written by the x sweep)
-    double t;                    // simulated time after the last completed step
+    double t;                    // simulated time in the reference's accounting: after each
+                                 // step it adds the dt of the NEXT step (src/update.cpp:167-168,
+                                 // timestep(W); t += dt)
     long long iter;              // completed steps
     unsigned long long wave[2];  // max(|u|+c) of the current/next state, as double bits
     int status;                  // bit 0: non-finite state detected
@@ -84,7 +86,19 @@ cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cud
 // the same sweeps with the reconstruction and the flux in single precision (sweep_mixed.cu)
 cudaError_t launch_sweep_mixed(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s);
 cudaError_t sweep_mixed_prepare();
-cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, cudaStream_t s);
+// ghost wrap of W; with finish_step also the clock update that closes a step:
+// iter += 1 and t += the dt of the next step (wave slot `slot`, or the fixed dt)
+cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, int slot,
+                        int dt_fixed_mode, double dt_fixed, cudaStream_t s);
+
+// dt = cfl*dx/max(|u|+c) from a wave-speed slot, or the fixed dt (src/update.cpp:1053)
+__device__ __forceinline__ double cfl_dt(const FieldConst& fc, const DevClock* c, int slot, int dt_fixed_mode,
+                                        double dt_fixed)
+{
+    if (dt_fixed_mode) return dt_fixed;
+    const double mw = __longlong_as_double((long long)c->wave[slot]);
+    return __ddiv_rn(__dmul_rn(fc.cfl, fc.dx), mw);
+}
 cudaError_t launch_wave_reduce(const double* W, const FieldConst& fc, DevClock* clock, int slot, cudaStream_t s);
 cudaError_t launch_flux_faces(const double* in, long long nfaces, double gam, int K, double dt, double dx,
                               double* F, cudaStream_t s);
@@ -120,6 +134,17 @@ cudaError_t launch_particles_heun(const double* const coefs[3], const SplineGrid
 struct StatsPartial {  // per-CTA partial sums of the PrintStats moments
     double v[16];
 };
+
+// particle properties (getParticleProp) and their statistics (GetParticleStats)
+constexpr int kPropCount = 41;
+constexpr int kSplineDensity = 0, kSplinePressure = 4, kSplinePlain = 5;   // launch_spline_source kinds (1..3 velocity)
+cudaError_t launch_spline_source(const double* src, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
+                                 int kind, double* coef, double* scratch, cudaStream_t s);
+cudaError_t launch_lap_nodes(const double* coef, const SplineGrid& g, const FieldConst& fc, double* out, cudaStream_t s);
+cudaError_t launch_particle_props(const double* const coefs[8], const SplineGrid& g, long long np, const double* py,
+                                  const double* px, const double* pz, double* props, cudaStream_t s);
+cudaError_t launch_particle_stats(const double* props, long long np, StatsPartial* partials, int nblocks, double* out6,
+                                  cudaStream_t s);
 cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const double* const coefs[3],
                          StatsPartial* partials, int nblocks, double* out16, cudaStream_t s);
 

@@ -72,7 +72,23 @@ __device__ void line_solve(const Src& f, int N, int periodic, const SplineTables
     }
 }
 
-// pass 0: velocity component q of W along axis 0 (y) -> out [M0][N1][N2]; one line (i, k)
+// Data of a spline at ghost-layout cell idx (generateSplines, src/update.cpp:1200-1210,1239-1241):
+// q = 1..3 velocity rho u_q / rho; q = kSrcDensity rho; q = kSrcPressure
+// (rho (gam-1)) (rho E / rho - |u|^2 / 2); q = kSrcPlain the array itself (one nt^3 component).
+constexpr int kSrcDensity = 0, kSrcPressure = 4, kSrcPlain = 5;
+
+__device__ __forceinline__ double spline_source(const double* __restrict__ W, long long nt3, double gm1, int q,
+                                                long long idx)
+{
+    if (q == kSrcDensity || q == kSrcPlain) return W[idx];
+    const double d = W[idx];
+    if (q != kSrcPressure) return __ddiv_rn(W[q * nt3 + idx], d);
+    const double u = __ddiv_rn(W[nt3 + idx], d), v = __ddiv_rn(W[2 * nt3 + idx], d), w = __ddiv_rn(W[3 * nt3 + idx], d);
+    const double vs = add(add(mul(u, u), mul(v, v)), mul(w, w));
+    return mul(mul(d, gm1), sub(__ddiv_rn(W[4 * nt3 + idx], d), mul(0.5, vs)));
+}
+
+// pass 0: the data of source q along axis 0 (y) -> out [M0][N1][N2]; one line (i, k)
 __device__ __forceinline__ void pass0_line(const double* __restrict__ W, const FieldConst& fc, const SplineGrid& g,
                                            const SplineTables& tb, int q, double* __restrict__ out, long long L)
 {
@@ -84,10 +100,7 @@ __device__ __forceinline__ void pass0_line(const double* __restrict__ W, const F
     const int i = (int)(L / N), k = (int)(L - (long long)i * N);
     const long long base = (long long)(i + off) * nt + (k + off);
     const long long sj = (long long)nt * nt;
-    auto f = [&](int j) {
-        const long long idx = (long long)(j + off) * sj + base;
-        return __ddiv_rn(W[q * nt3 + idx], W[idx]);   // u = rho u / rho, src/update.cpp:1239-1241
-    };
+    auto f = [&](int j) { return spline_source(W, nt3, fc.gm1, q, (long long)(j + off) * sj + base); };
     line_solve(f, N, g.periodic, tb, out + L, lines);
 }
 
@@ -325,6 +338,209 @@ __device__ __forceinline__ void eval3(const double* const* coefs, const SplineGr
 struct Coefs3 {
     const double* c[3];
 };
+
+// ---------------------------------------------- values, gradients, Hessians --
+// eval_UBspline_3d_d_vg / _vgl / _vgh as the CPU oracle evaluates them: basis
+// weights w, first derivatives d and second derivatives h per axis, the 4x4x4
+// window contracted along axis 2, then 1, then 0, every sum left to right.
+struct BasisFull {
+    double w[4], d[4], h[4];
+};
+
+__device__ __forceinline__ BasisFull basis_full(double t, double dinv)
+{
+    const double t2 = mul(t, t), t3 = mul(t2, t), s = sub(1.0, t);
+    const double c = 1.0 / 6.0;
+    BasisFull b;
+    b.w[0] = mul(c, mul(mul(s, s), s));
+    b.w[1] = mul(c, add(sub(mul(3.0, t3), mul(6.0, t2)), 4.0));
+    b.w[2] = mul(c, add(add(add(mul(-3.0, t3), mul(3.0, t2)), mul(3.0, t)), 1.0));
+    b.w[3] = mul(c, t3);
+    b.d[0] = mul(mul(-0.5, mul(s, s)), dinv);
+    b.d[1] = mul(mul(0.5, sub(mul(3.0, t2), mul(4.0, t))), dinv);
+    b.d[2] = mul(mul(0.5, add(add(mul(-3.0, t2), mul(2.0, t)), 1.0)), dinv);
+    b.d[3] = mul(mul(0.5, t2), dinv);
+    const double d2 = mul(dinv, dinv);
+    b.h[0] = mul(s, d2);
+    b.h[1] = mul(sub(mul(3.0, t), 2.0), d2);
+    b.h[2] = mul(add(mul(-3.0, t), 1.0), d2);
+    b.h[3] = mul(t, d2);
+    return b;
+}
+
+__device__ __forceinline__ double dot4(const double a[4], const double* r)
+{
+    return add(add(add(mul(a[0], r[0]), mul(a[1], r[1])), mul(a[2], r[2])), mul(a[3], r[3]));
+}
+
+__device__ __forceinline__ double dot4(const double a[4], double r0, double r1, double r2, double r3)
+{
+    return add(add(add(mul(a[0], r0), mul(a[1], r1)), mul(a[2], r2)), mul(a[3], r3));
+}
+
+struct SplineVal {
+    double v, g[3], lap, h[6];   // h: 00 01 02 11 12 22
+};
+
+// WHAT 1: value + gradient; 2: + Laplacian; 3: + Hessian
+template <int WHAT>
+__device__ __forceinline__ SplineVal spline_eval(const double* __restrict__ C, const SplineGrid& g, double a, double b,
+                                                 double c)
+{
+    double ta, tb, tc;
+    const int ia = locate(g, a, ta), ib = locate(g, b, tb), ic = locate(g, c, tc);
+    const BasisFull A = basis_full(ta, g.dinv), B = basis_full(tb, g.dinv), Z = basis_full(tc, g.dinv);
+    const long long M = g.npts + g.pad;
+    double v = 0, g0 = 0, g1 = 0, g2 = 0, h00 = 0, h01 = 0, h02 = 0, h11 = 0, h12 = 0, h22 = 0;
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        double cw[4], cd[4], ch[4];
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const double* row = C + ((long long)(ia + x) * M + (ib + y)) * M + ic;
+            const double r0 = row[0], r1 = row[1], r2 = row[2], r3 = row[3];
+            cw[y] = dot4(Z.w, r0, r1, r2, r3);
+            cd[y] = dot4(Z.d, r0, r1, r2, r3);
+            ch[y] = (WHAT >= 2) ? dot4(Z.h, r0, r1, r2, r3) : 0.0;
+        }
+        const double bw = dot4(B.w, cw), bd = dot4(B.d, cw), bwd = dot4(B.w, cd);
+        v = add(v, mul(A.w[x], bw));
+        g0 = add(g0, mul(A.d[x], bw));
+        g1 = add(g1, mul(A.w[x], bd));
+        g2 = add(g2, mul(A.w[x], bwd));
+        if (WHAT >= 2) {
+            const double bh = dot4(B.h, cw), bwh = dot4(B.w, ch);
+            h00 = add(h00, mul(A.h[x], bw));
+            h11 = add(h11, mul(A.w[x], bh));
+            h22 = add(h22, mul(A.w[x], bwh));
+        }
+        if (WHAT == 3) {
+            const double bdd = dot4(B.d, cd);
+            h01 = add(h01, mul(A.d[x], bd));
+            h02 = add(h02, mul(A.d[x], bwd));
+            h12 = add(h12, mul(A.w[x], bdd));
+        }
+    }
+    SplineVal r;
+    r.v = v;
+    r.g[0] = g0;
+    r.g[1] = g1;
+    r.g[2] = g2;
+    r.lap = (WHAT == 2) ? add(add(h00, h11), h22) : 0.0;
+    r.h[0] = h00;
+    r.h[1] = h01;
+    r.h[2] = h02;
+    r.h[3] = h11;
+    r.h[4] = h12;
+    r.h[5] = h22;
+    return r;
+}
+
+// Laplacian of a velocity spline at every spline node, written at the node's
+// ghost-layout cell (generateSplines, src/update.cpp:1217-1228): node (j, i, k)
+// sits at ((j - 3) dx + dx/2, ...) on the reference grid.  The reference's
+// loops visit interior nodes only; its ghost nodes keep the zeros of a fresh
+// allocation and are splined as zeros, which this reproduces.
+__global__ void lap_nodes_kernel(const double* __restrict__ C, SplineGrid g, FieldConst fc, double* __restrict__ out)
+{
+    const int N = g.npts, nt = fc.nt, off = g.periodic ? 3 : 0;
+    const long long total = (long long)N * N * N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(e / ((long long)N * N)), i = (int)((e / N) % N), k = (int)(e % N);
+        const int J = j + off, I = i + off, K = k + off;
+        const long long o = ((long long)J * nt + I) * nt + K;
+        if (J < 3 || J >= nt - 3 || I < 3 || I >= nt - 3 || K < 3 || K >= nt - 3) {
+            out[o] = 0.0;
+            continue;
+        }
+        const double hx = mul(0.5, fc.dx);
+        const double y = add(mul((double)(J - 3), fc.dx), hx);
+        const double x = add(mul((double)(I - 3), fc.dx), hx);
+        const double z = add(mul((double)(K - 3), fc.dx), hx);
+        out[o] = spline_eval<2>(C, g, y, x, z).lap;
+    }
+}
+
+struct Coefs8 {
+    const double* c[8];   // rho, u, v, w, p, lap u, lap v, lap w
+};
+
+// getParticleProp (src/ParticleTrack.cpp:99-113) for every particle; props is
+// SoA [kPropCount][np] in the order of the property table of include/gkm.h.
+__global__ void particle_props_kernel(Coefs8 cf, SplineGrid g, long long np, const double* __restrict__ py,
+                                      const double* __restrict__ px, const double* __restrict__ pz,
+                                      double* __restrict__ props)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        const double a = py[p], b = px[p], c = pz[p];
+        double* o = props + p;
+        auto put = [&](int slot, double v) { o[(long long)slot * np] = v; };
+        const SplineVal d = spline_eval<1>(cf.c[0], g, a, b, c);
+        put(0, d.v);
+        for (int q = 0; q < 3; q++) put(1 + q, d.g[q]);
+        for (int f = 0; f < 3; f++) {
+            const SplineVal u = spline_eval<1>(cf.c[1 + f], g, a, b, c);
+            put(4 + f, u.v);
+            for (int q = 0; q < 3; q++) put(7 + 3 * f + q, u.g[q]);
+        }
+        const SplineVal P = spline_eval<3>(cf.c[4], g, a, b, c);
+        put(16, P.v);
+        for (int q = 0; q < 3; q++) put(17 + q, P.g[q]);
+        const int hmap[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        for (int q = 0; q < 9; q++) put(20 + q, P.h[hmap[q]]);
+        for (int f = 0; f < 3; f++) {
+            const SplineVal l = spline_eval<1>(cf.c[5 + f], g, a, b, c);
+            put(29 + f, l.v);
+            for (int q = 0; q < 3; q++) put(32 + 3 * f + q, l.g[q]);
+        }
+    }
+}
+
+// GetParticleStats (src/update.cpp:1111-1162): per-CTA sums of U.U, S_ij S_ij,
+// (du/dx)^2, (du/dx)^3, (dw/dz)^2, (dw/dz)^3 over the particles (gradients are
+// (d/dy, d/dx, d/dz) in the property table)
+__global__ void particle_stats_kernel(const double* __restrict__ props, long long np, StatsPartial* __restrict__ part)
+{
+    __shared__ double red[6][32];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        auto P = [&](int slot) { return props[(long long)slot * np + p]; };
+        const double U0 = P(4), U1 = P(5), U2 = P(6);
+        const double dudx = P(8), dvdx = P(11), dwdx = P(14);
+        const double dudy = P(7), dvdy = P(10), dwdy = P(13);
+        const double dudz = P(9), dvdz = P(12), dwdz = P(15);
+        acc[0] += U0 * U0 + U1 * U1 + U2 * U2;
+        acc[1] += dudx * dudx + 0.5 * ((dudy + dvdx) * (dudy + dvdx)) + 0.5 * ((dudz + dwdx) * (dudz + dwdx)) +
+                  0.5 * ((dwdy + dvdz) * (dwdy + dvdz)) + dvdy * dvdy + dwdz * dwdz;
+        acc[2] += dudx * dudx;
+        acc[3] += dudx * dudx * dudx;
+        acc[4] += dwdz * dwdz;
+        acc[5] += dwdz * dwdz * dwdz;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+        double v = acc[s];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[s][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 16) {
+        double v = 0.0;
+        if (threadIdx.x < 6)
+            for (int w2 = 0; w2 < (int)(blockDim.x >> 5); w2++) v += red[threadIdx.x][w2];
+        part[blockIdx.x].v[threadIdx.x] = v;
+    }
+}
+
+__global__ void particle_stats_finish(const StatsPartial* __restrict__ part, int nblocks, double* __restrict__ out)
+{
+    const int s = threadIdx.x;
+    if (s >= 6) return;
+    double v = 0.0;
+    for (int b = 0; b < nblocks; b++) v += part[b].v[s];
+    out[s] = v;
+}
 
 __global__ void particles_eval_kernel(Coefs3 cf, SplineGrid g, long long np, const double* __restrict__ py,
                                       const double* __restrict__ px, const double* __restrict__ pz,
@@ -630,6 +846,38 @@ cudaError_t launch_ensemble_heun(const MemberDev* mem, const long long* off, int
 {
     if (total <= 0) return cudaSuccess;
     return grid_launch(ensemble_heun_kernel, total, 128, s, mem, off, nm);
+}
+
+// spline of an arbitrary source (spline_source kinds) with caller scratch
+cudaError_t launch_spline_source(const double* src, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
+                                 int kind, double* coef, double* scratch, cudaStream_t s)
+{
+    return launch_spline_component(src, fc, g, tb, kind, coef, scratch, s);
+}
+
+cudaError_t launch_lap_nodes(const double* coef, const SplineGrid& g, const FieldConst& fc, double* out, cudaStream_t s)
+{
+    const long long N = g.npts;
+    return grid_launch(lap_nodes_kernel, N * N * N, 128, s, coef, g, fc, out);
+}
+
+cudaError_t launch_particle_props(const double* const coefs[8], const SplineGrid& g, long long np, const double* py,
+                                  const double* px, const double* pz, double* props, cudaStream_t s)
+{
+    if (np <= 0) return cudaSuccess;
+    Coefs8 cf;
+    for (int q = 0; q < 8; q++) cf.c[q] = coefs[q];
+    return grid_launch(particle_props_kernel, np, 128, s, cf, g, np, py, px, pz, props);
+}
+
+cudaError_t launch_particle_stats(const double* props, long long np, StatsPartial* partials, int nblocks, double* out6,
+                                  cudaStream_t s)
+{
+    particle_stats_kernel<<<nblocks, 256, 0, s>>>(props, np, partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    particle_stats_finish<<<1, 32, 0, s>>>(partials, nblocks, out6);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np, const double* py,

@@ -22,11 +22,13 @@ namespace {
 using sweep_detail::block_max;
 using sweep_detail::wave_speed;
 
-__global__ void halo_kernel(double* __restrict__ W, FieldConst fc, DevClock* clock, int finish_step)
+__global__ void halo_kernel(double* __restrict__ W, FieldConst fc, DevClock* clock, int finish_step, int slot,
+                            int dt_fixed_mode, double dt_fixed)
 {
     const long long total = fc.nt3 - (long long)fc.n * fc.n * fc.n;
     if (finish_step && blockIdx.x == 0 && threadIdx.x == 0) {
-        clock->t += clock->dt;   // src/update.cpp:168-169
+        // src/update.cpp:167-169: timestep(W) of the new state, then t += dt
+        clock->t += cfl_dt(fc, clock, slot, dt_fixed_mode, dt_fixed);
         clock->iter += 1;
     }
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
@@ -143,7 +145,7 @@ __global__ void ensemble_halo_kernel(const MemberDev* __restrict__ mem, const lo
         const MemberDev& md = mem[m];
         const long long local = g - off[m];
         if (finish_step && local == 0) {
-            md.clock->t += md.clock->dt;
+            md.clock->t += cfl_dt(md.fc, md.clock, buf, md.dt_fixed_mode, md.dt_fixed);   // src/update.cpp:167-169
             md.clock->iter += 1;
         }
         halo_cell(md.buf[buf], md.fc, local);
@@ -197,12 +199,13 @@ cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cud
     return launch_one<2, SweepTile64a>(a, nseg, s);
 }
 
-cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, cudaStream_t s)
+cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, int slot,
+                        int dt_fixed_mode, double dt_fixed, cudaStream_t s)
 {
     long long total = (long long)fc.nt * fc.nt * fc.nt - (long long)fc.n * fc.n * fc.n;
     int blocks = (int)((total + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    halo_kernel<<<blocks, 256, 0, s>>>(W, fc, clock, finish_step);
+    halo_kernel<<<blocks, 256, 0, s>>>(W, fc, clock, finish_step, slot, dt_fixed_mode, dt_fixed);
     return cudaGetLastError();
 }
 

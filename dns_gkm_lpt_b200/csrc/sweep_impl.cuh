@@ -100,9 +100,7 @@ __device__ __forceinline__ double wave_speed(const double w[5], double gam, doub
 
 __device__ __forceinline__ double step_dt(const SweepArgs& a)
 {
-    if (a.dt_fixed_mode) return a.dt_fixed;
-    double mw = __longlong_as_double((long long)a.clock->wave[a.parity]);
-    return __ddiv_rn(__dmul_rn(a.fc.cfl, a.fc.dx), mw);   // dt = cfl*dx/maxVAL, src/update.cpp:1053
+    return cfl_dt(a.fc, a.clock, a.parity, a.dt_fixed_mode, a.dt_fixed);
 }
 
 __device__ __forceinline__ double block_max(double v, double* red)

@@ -173,3 +173,106 @@ def read_reference_params(directory: str) -> Params:
 def particles_to_reference_order(xyz: np.ndarray) -> np.ndarray:
     """(x, y, z) -> the reference's particle position order (y, x, z) (ParticleTrack.cpp:15-17)."""
     return np.ascontiguousarray(xyz[:, [1, 0, 2]])
+
+
+def make_state_device(n: int, Mt: float, Re: float, seed: int, device="cuda", k0: float = 4.0, kcmin: float = 1.0,
+                      kcmax: float = 8.0, gam: float = 1.4, rho0: float = 1.0, T0: float = 300.0, rand=None):
+    """The make_field recipe computed with torch (cuFFT on a GPU), returning
+    (params, W) with W the conserved state already in the reference layout,
+    a (5, n+6, n+6, n+6) float64 tensor on ``device`` whose ghosts are left
+    for gkm_upload_state to wrap.  For the large grids (512^3, 1024^3) the
+    NumPy path would need tens to hundreds of GB of host memory.
+
+    The random u, v, w come from torch's generator seeded with ``seed`` (a
+    different stream from NumPy's), unless ``rand`` supplies the three
+    (n, n, n) arrays; with NumPy's draws it reproduces make_field to rounding.
+    Real-to-complex transforms halve the spectral memory: the projection and
+    the shell rescale keep the spectrum Hermitian and the shell (|k| <= 8)
+    never reaches the Nyquist planes for n >= 32, so irfftn equals the real
+    part of the full inverse transform.
+    """
+    import torch
+
+    dev = torch.device(device)
+    f64 = torch.float64
+    Np = float(n) ** 3
+    A = np.sqrt(2.0 / np.pi) * (16.0 / 3.0) * Mt ** 2 / k0 ** 5
+    kf = torch.tensor(_kfft(n), dtype=f64, device=dev)
+    k2 = kf.view(n, 1, 1)                       # dim 0 (y) pairs with v
+    k1 = kf.view(1, n, 1)                       # dim 1 (x) pairs with u
+    k3 = kf[: n // 2 + 1].view(1, 1, n // 2 + 1)  # dim 2 (z, half spectrum) pairs with w
+    if rand is None:
+        g = torch.Generator(device=dev)
+        g.manual_seed(int(seed))
+    spec = []
+    for c in range(3):
+        r = (torch.as_tensor(rand[c], dtype=f64, device=dev) if rand is not None
+             else torch.rand((n, n, n), generator=g, dtype=f64, device=dev))
+        spec.append(torch.fft.rfftn(r))
+        del r
+    uk, vk, wk = spec
+    del spec
+    ksq = (k1 * k1 + k2 * k2 + k3 * k3).clamp_min(1e-14)
+    kdot = uk * k1
+    kdot += vk * k2
+    kdot += wk * k3
+    kdot /= ksq
+    uk -= kdot * k1
+    vk -= kdot * k2
+    wk -= kdot * k3
+    del kdot
+    kk = ksq.sqrt_()                            # ksq is not needed any more
+    del ksq
+    shell = (kk >= kcmin) & (kk <= kcmax)
+    ee = A * kk ** 4 * torch.exp(-2.0 * (kk / k0) ** 2) * Np ** 2
+    ee = torch.where(shell, ee / (4.0 * np.pi * torch.where(shell, kk, torch.ones_like(kk)) ** 2),
+                     torch.zeros_like(ee))
+    umag2 = uk.real ** 2 + uk.imag ** 2
+    umag2 += vk.real ** 2 + vk.imag ** 2
+    umag2 += wk.real ** 2 + wk.imag ** 2
+    ok = shell & (umag2 > 0)
+    fac = torch.where(ok, torch.sqrt(ee / torch.where(umag2 > 0, umag2, torch.ones_like(umag2))),
+                      torch.zeros_like(ee))
+    del ee, umag2, ok, shell, kk
+    fac /= Np
+    vel = []
+    for sk in (uk, vk, wk):
+        sk *= fac
+        vel.append(torch.fft.irfftn(sk, s=(n, n, n)))
+    del uk, vk, wk, fac
+    u, v, w = vel
+    del vel
+
+    p0 = rho0 * R_GAS * T0
+    ek0 = 0.5 * float(((u * u).mean() + (v * v).mean() + (w * w).mean()).item())
+    M = np.sqrt(2 * ek0) / np.sqrt(gam * p0 / rho0)
+    eta = Mt / M
+    for a in (u, v, w):
+        a *= eta
+    ek0 = 0.5 * float(((u * u).mean() + (v * v).mean() + (w * w).mean()).item())
+    Mt_out = np.sqrt(2 * ek0) / np.sqrt(gam * p0 / rho0)
+    dx = 2 * np.pi / n
+    sqdu = 0.0
+    for a in (u, v, w):
+        for ax in (1, 0, 2):
+            d = (torch.roll(a, -1, ax) - torch.roll(a, 1, ax)) * (0.5 / dx)
+            sqdu += float((d * d).mean().item())
+            del d
+    mu = 2 * ek0 * np.sqrt(5 / (3 * sqdu)) / Re
+    lam = np.sqrt(10 * ek0 / sqdu)
+    urms = np.sqrt(2 * ek0 / 3)
+    params = Params(n=n, gam=gam, den0=rho0, Mt=float(Mt_out), Re=float(Re), mu0=float(mu), p0=p0,
+                    t0=float(lam / urms))
+    nt = n + 6
+    W = torch.zeros((5, nt, nt, nt), dtype=f64, device=dev)
+    inner = (slice(3, nt - 3),) * 3
+    W[0][inner] = rho0
+    W[1][inner] = u * rho0
+    W[2][inner] = v * rho0
+    W[3][inner] = w * rho0
+    e = u * u
+    e += v * v
+    e += w * w
+    del u, v, w
+    W[4][inner] = rho0 * (p0 / (rho0 * (gam - 1.0))) + 0.5 * rho0 * e
+    return params, W

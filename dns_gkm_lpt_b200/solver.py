@@ -41,7 +41,14 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_dp)
 
 
-def _w5(W: np.ndarray):
+def _w5(W):
+    """Five component pointers of a (5, nt, nt, nt) float64 array: a NumPy array
+    (host) or a CUDA tensor (device; the C ABI copies either way)."""
+    if hasattr(W, "data_ptr"):   # torch tensor
+        import torch
+        if W.dtype != torch.float64 or not W.is_contiguous() or W.dim() != 4 or W.shape[0] != 5:
+            raise ValueError("W must be a contiguous float64 tensor of shape (5, nt, nt, nt)")
+        return (_dp * 5)(*[C.cast(C.c_void_p(W[q].data_ptr()), _dp) for q in range(5)])
     if W.dtype != np.float64 or not W.flags.c_contiguous or W.ndim != 4 or W.shape[0] != 5:
         raise ValueError("W must be a C-contiguous float64 array of shape (5, nt, nt, nt)")
     return (_dp * 5)(*[_ptr(W[q]) for q in range(5)])
@@ -113,7 +120,8 @@ class Solver:
     def upload_state(self, W: np.ndarray) -> None:
         self._check(self.L.gkm_upload_state(self.h, _w5(W)))
 
-    def download_state(self, out: np.ndarray | None = None) -> np.ndarray:
+    def download_state(self, out=None):
+        """Current state (ghosts wrapped) into ``out`` (NumPy array or CUDA tensor) or a new NumPy array."""
         out = np.empty((5, self.nt, self.nt, self.nt)) if out is None else out
         self._check(self.L.gkm_download_state(self.h, _w5(out)))
         return out
@@ -202,6 +210,47 @@ class Solver:
         st = _capi.GkmStats()
         self._check(self.L.gkm_stats_compute(self.h, C.byref(st)))
         return st.as_dict()
+
+    # -- particle properties and output files ------------------------------------
+    def particle_props(self) -> np.ndarray:
+        """getParticleProp for every particle: (np, 41), columns _capi.PROP_NAMES."""
+        out = np.empty((self.np, _capi.PROP_COUNT))
+        self._check(self.L.gkm_particle_props(self.h, _ptr(out) if self.np else None))
+        return out
+
+    def particle_stats(self) -> dict:
+        """GetParticleStats: particle TKE, SijSij, SKEWu, SKEWw."""
+        st = _capi.GkmParticleStats()
+        self._check(self.L.gkm_particle_stats_compute(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def write_field(self, path: str) -> None:
+        self._check(self.L.gkm_write_field(self.h, path.encode()))
+
+    def write_particles(self, path: str) -> None:
+        self._check(self.L.gkm_write_particles(self.h, path.encode()))
+
+    def write_time(self, path: str) -> None:
+        self._check(self.L.gkm_write_time(self.h, path.encode()))
+
+    def write_reinit(self, path: str) -> None:
+        self._check(self.L.gkm_write_reinit(self.h, path.encode()))
+
+    def write_outputs(self, directory: str, iteration: int, rank: int = 0) -> dict:
+        """The files the reference writes at an output iteration, under its own names
+        (Results/Field, Results/Particles, Results/Time, InitialCondition)."""
+        import os
+        paths = {"field": os.path.join(directory, "Results", "Field", f"Field_{rank}_{iteration}"),
+                 "particles": os.path.join(directory, "Results", "Particles", f"P_{rank}_{iteration}"),
+                 "time": os.path.join(directory, "Results", "Time", f"T_{iteration}"),
+                 "reinit": os.path.join(directory, "InitialCondition", "Init000")}
+        for p in paths.values():
+            os.makedirs(os.path.dirname(p), exist_ok=True)
+        self.write_field(paths["field"])
+        self.write_reinit(paths["reinit"])
+        self.write_particles(paths["particles"])
+        self.write_time(paths["time"])
+        return paths
 
 
 class Ensemble:

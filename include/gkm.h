@@ -112,10 +112,12 @@ int gkm_nt(const gkm_handle* h);
 /* Host -> device copy of the conserved state in the reference layout, then
  * the periodic ghost wrap and the dt reduction.  Replaces the H2D half of
  * evolve() (src/GPUupdate.cu:89-93) and Initialize_DHIT's result
- * (src/FlowField.cpp:60-114).  Ghost values in W may be stale. */
+ * (src/FlowField.cpp:60-114).  Ghost values in W may be stale.  The W[q]
+ * may also be device pointers (unified addressing picks the copy direction),
+ * e.g. an initial field generated on the GPU. */
 gkm_status gkm_upload_state(gkm_handle* h, const double* const W[5]);
 /* Device -> host copy (ghosts included, already wrapped); D2H half of evolve()
- * (src/GPUupdate.cu:209-213). */
+ * (src/GPUupdate.cu:209-213).  Device destination pointers work as well. */
 gkm_status gkm_download_state(gkm_handle* h, double* const W[5]);
 
 /* timestep(W) (src/update.cpp:1031-1054): dt = cfl*dx / max(|u| + c) of the
@@ -215,6 +217,56 @@ gkm_status gkm_stats_compute(gkm_handle* h, gkm_stats* out);
  * Results equal gkm_generate_splines + gkm_spline_coefs bit for bit. */
 gkm_status gkm_spline_build_noalloc(const double* W, int32_t n, int32_t spline_mode, int32_t component,
                                     double* coefs, void* stream);
+
+/* ----------------------------------------------------- particle properties
+ *
+ * getParticleProp (src/ParticleTrack.cpp:99-113) for every particle at its
+ * current position: the reference's eight splines of the current state
+ * (generateSplines, src/update.cpp:1200-1233: rho, u, v, w, p, and the
+ * Laplacians of u, v, w evaluated at every spline node and splined again),
+ * then value + gradient of each (value + gradient + Hessian for p).  props
+ * receives np x GKM_PROP_COUNT doubles, particle-major, in upload order:
+ *   0 rho            1..3 grad rho           4..6 u, v, w
+ *   7..9 grad u      10..12 grad v           13..15 grad w
+ *   16 p             17..19 grad p           20..28 Hessian of p (row-major)
+ *   29..31 lap u, lap v, lap w               32..40 grad lap u, v, w
+ * Every gradient is (d/dy, d/dx, d/dz), the spline axis order (members DEN,
+ * gradD, U, gradU, ..., hessP, lapU, ..., gradLapW of class Particle,
+ * src/ParticleTrack.h:20-21).  The five extra splines (5 x (N+P)^3 doubles)
+ * and an nt^3 node array are allocated on first use. */
+#define GKM_PROP_COUNT 41
+gkm_status gkm_particle_props(gkm_handle* h, double* props);
+
+/* GetParticleStats (src/update.cpp:1111-1162) from the properties above:
+ * particle-averaged |U|^2, S_ij S_ij, and the skewness of du/dx and dw/dz. */
+typedef struct gkm_particle_stats {
+    double TKE, SijSij, SKEWu, SKEWw;
+    int64_t count;
+} gkm_particle_stats;
+gkm_status gkm_particle_stats_compute(gkm_handle* h, gkm_particle_stats* out);
+
+/* ------------------------------------------------------------ output files
+ *
+ * The reference's output formats written from the current device state, so
+ * its post-processing and restart readers take them unchanged.  The caller
+ * picks the path; the reference's own names are Results/Field/Field_<rank>_
+ * <iter>, Results/Particles/P_<rank>_<iter>, Results/Time/T_<iter> and
+ * InitialCondition/Init<py><px><pz> (000 for the single cube). */
+
+/* writeField (src/update.cpp:1324-1339): per interior cell, y-major then x
+ * then z, "%d %d %d %.15e x5" with the x, y, z indices and rho, u, v, w, p. */
+gkm_status gkm_write_field(gkm_handle* h, const char* path);
+/* writeParticleData (src/update.cpp:1341-1368), one line per particle in
+ * upload order (tag = upload index): position, rho, U, p and the gradients and
+ * Hessian of gkm_particle_props in the reference's column order. */
+gkm_status gkm_write_particles(gkm_handle* h, const char* path);
+/* The time file of writeParticleData (src/update.cpp:1370-1378): t, the dt of
+ * the coming step, t0 as "%.15e %.15e %.15e". */
+gkm_status gkm_write_time(gkm_handle* h, const char* path);
+/* WriteReInit (src/update.cpp:1381-1422): u, v, w, rho, p of the interior
+ * cells, each n^3 doubles in MATLAB (column-major) order, the initial-field
+ * format that Initialize_DHIT reads (src/FlowField.cpp:60-114). */
+gkm_status gkm_write_reinit(gkm_handle* h, const char* path);
 
 /* ---------------------------------------------------- single-call numerics */
 

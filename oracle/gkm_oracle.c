@@ -937,6 +937,133 @@ static void orc_build_field_splines(const orc_params *p, double *const W[5], int
 	free(f);
 }
 
+/* one more spline of the field from an nt^3 (ghost-layout) array; nodes as orc_build_field_splines */
+static void orc_build_array_spline(const orc_params *p, const double *a, int spline_mode, orc_spline *s)
+{
+	const int nt = p->nt, n = p->n;
+	const int periodic = spline_mode == 1;
+	const int npts = periodic ? n : nt;
+	const int P = orc_spline_pad(periodic);
+	const long M = (long)(npts + P) * (npts + P) * (npts + P);
+	double start, dinv;
+	if (periodic)
+		orc_grid_periodic(p, &start, &dinv);
+	else
+		orc_grid_natural_ghost3(p, &start, &dinv);
+	double *f = (double *)malloc(sizeof(double) * (size_t)npts * npts * npts);
+	long m = 0;
+	for (int j = 0; j < nt; j++)
+		for (int i = 0; i < nt; i++)
+			for (int k = 0; k < nt; k++)
+			{
+				if (periodic && (j < 3 || j >= n + 3 || i < 3 || i >= n + 3 || k < 3 || k >= n + 3))
+					continue;
+				f[m++] = a[((long)j * nt + i) * nt + k];
+			}
+	s->coefs = (double *)malloc(sizeof(double) * (size_t)M);
+	s->periodic = periodic;
+	for (int ax = 0; ax < 3; ax++)
+	{
+		s->n[ax] = npts;
+		s->start[ax] = start;
+		s->dinv[ax] = dinv;
+	}
+	orc_spline3d_build(f, s->n, periodic, s->coefs, NULL);
+	free(f);
+}
+
+/* reference src/update.cpp:1200-1233 (the eight splines) and
+ * src/ParticleTrack.cpp:99-113 (getParticleProp); out: np x 41, the
+ * property table of include/gkm.h */
+void orc_particle_props(const orc_params *p, double *const W[5], int spline_mode, long np, const double *pos,
+						double *out)
+{
+	const int nt = p->nt, n = p->n;
+	const long Nt = (long)nt * nt * nt;
+	const int periodic = spline_mode == 1;
+	orc_spline s[8];
+	memset(s, 0, sizeof(s));
+	orc_build_field_splines(p, W, spline_mode, s, 1);   /* rho, u, v, w */
+	double *a = (double *)malloc(sizeof(double) * (size_t)Nt);
+	/* p = (den (gam - 1)) (W4 / den - 0.5 Vsqr), src/update.cpp:1202-1209 */
+	for (long c = 0; c < Nt; c++)
+	{
+		double den = W[0][c];
+		double u = W[1][c] / den, v = W[2][c] / den, w = W[3][c] / den;
+		double Vsqr = u * u + v * v + w * w;
+		a[c] = (den * (p->gam - 1)) * (W[4][c] / den - 0.5 * Vsqr);
+	}
+	orc_build_array_spline(p, a, spline_mode, &s[4]);
+	/* Laplacians at the nodes, src/update.cpp:1217-1228: the reference's For
+	 * loops visit the interior nodes only; the ghost nodes of its (freshly
+	 * allocated) arrays stay zero and enter the natural_ghost3 splines as such */
+	for (int f = 0; f < 3; f++)
+	{
+		for (int j = 0; j < nt; j++)
+			for (int i = 0; i < nt; i++)
+				for (int k = 0; k < nt; k++)
+				{
+					long c = ((long)j * nt + i) * nt + k;
+					if (j < 3 || j >= n + 3 || i < 3 || i >= n + 3 || k < 3 || k >= n + 3)
+					{
+						a[c] = 0.0;
+						continue;
+					}
+					double y = (j - 3) * p->dx + 0.5 * p->dx;
+					double x = (i - 3) * p->dx + 0.5 * p->dx;
+					double z = (k - 3) * p->dx + 0.5 * p->dx;
+					double v, g[3], h[9];
+					orc_spline3d_eval(&s[1 + f], y, x, z, 2, &v, g, &a[c], h);
+				}
+		orc_build_array_spline(p, a, spline_mode, &s[5 + f]);
+	}
+	free(a);
+	for (long q = 0; q < np; q++)
+	{
+		const double y = pos[3 * q], x = pos[3 * q + 1], z = pos[3 * q + 2];
+		double *o = out + 41 * q;
+		double l, h[9];
+		orc_spline3d_eval(&s[0], y, x, z, 1, &o[0], &o[1], &l, h);
+		for (int f = 0; f < 3; f++)
+			orc_spline3d_eval(&s[1 + f], y, x, z, 1, &o[4 + f], &o[7 + 3 * f], &l, h);
+		orc_spline3d_eval(&s[4], y, x, z, 3, &o[16], &o[17], &l, &o[20]);
+		for (int f = 0; f < 3; f++)
+			orc_spline3d_eval(&s[5 + f], y, x, z, 1, &o[29 + f], &o[32 + 3 * f], &l, h);
+	}
+	for (int q = 0; q < 8; q++)
+		free(s[q].coefs);
+}
+
+/* reference src/update.cpp:1111-1162 on a property table */
+void orc_particle_stats(const double *props, long np, double out[4])
+{
+	double tke = 0, sij = 0, ux2 = 0, ux3 = 0, wz2 = 0, wz3 = 0;
+	for (long q = 0; q < np; q++)
+	{
+		const double *o = props + 41 * q;
+		tke += (o[4] * o[4] + o[5] * o[5] + o[6] * o[6]);
+		double dudx = o[8], dvdx = o[11], dwdx = o[14];
+		double dudy = o[7], dvdy = o[10], dwdy = o[13];
+		double dudz = o[9], dvdz = o[12], dwdz = o[15];
+		sij += (dudx * dudx + 0.5 * pow(dudy + dvdx, 2) + 0.5 * pow(dudz + dwdx, 2) + 0.5 * pow(dwdy + dvdz, 2) +
+				dvdy * dvdy + dwdz * dwdz);
+		ux2 += dudx * dudx;
+		ux3 += dudx * dudx * dudx;
+		wz2 += dwdz * dwdz;
+		wz3 += dwdz * dwdz * dwdz;
+	}
+	tke /= np;
+	sij /= np;
+	ux2 /= np;
+	ux3 /= np;
+	wz2 /= np;
+	wz3 /= np;
+	out[0] = tke;
+	out[1] = sij;
+	out[2] = ux3 / pow(ux2, 1.5);
+	out[3] = wz3 / pow(wz2, 1.5);
+}
+
 static void orc_free_splines(orc_spline s[4])
 {
 	for (int q = 0; q < 4; q++)

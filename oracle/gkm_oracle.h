@@ -101,6 +101,14 @@ typedef struct
 void orc_print_stats(const orc_params *p, double *const W[5], const orc_spline *sden,
 					 const orc_spline *su, const orc_spline *sv, const orc_spline *sw, orc_stats *out);
 
+/* ---- particle properties (src/ParticleTrack.cpp:99-113 with the eight splines
+ * of src/update.cpp:1200-1233) and their statistics (src/update.cpp:1111-1162).
+ * W: 5 arrays nt^3 with valid ghosts; pos: np*3 (y,x,z); out: np*41 (the
+ * property table of include/gkm.h); stats: TKE, SijSij, SKEWu, SKEWw. */
+void orc_particle_props(const orc_params *p, double *const W[5], int spline_mode, long np, const double *pos,
+						double *out);
+void orc_particle_stats(const double *props, long np, double out[4]);
+
 /* ---- whole-run driver mirroring Evolve's loop body (src/update.cpp:124-170) ----
  * mode bits: spline_mode 0 natural_ghost3 / 1 periodic.
  * W: 5 arrays nt^3 (interior filled; ghosts are refreshed here).

@@ -87,6 +87,8 @@ class Oracle:
         L.orc_grid_periodic.argtypes = [C.POINTER(OrcParams), _dp, _dp]
         L.orc_print_stats.argtypes = [C.POINTER(OrcParams), _dp * 5] + [C.POINTER(OrcSpline)] * 4 + [
             C.POINTER(OrcStats)]
+        L.orc_particle_props.argtypes = [C.POINTER(OrcParams), _dp * 5, C.c_int, C.c_long, _dp, _dp]
+        L.orc_particle_stats.argtypes = [_dp, C.c_long, _dp]
 
     # -- parameters ----------------------------------------------------------
     def params(self, P, cfl: float, visc_law: int = 0) -> OrcParams:
@@ -143,6 +145,20 @@ class Oracle:
                             _ptr(pos) if npart else None, _ptr(U) if npart else None, _ptr(dts),
                             st if stats else None)
         return {"dt": dts[:nsteps], "pos": pos, "U": U, "stats": [st[i].as_dict() for i in range(ns)]}
+
+    def particle_props(self, p: OrcParams, W: np.ndarray, pos: np.ndarray, spline_mode: int = 0) -> np.ndarray:
+        """getParticleProp with the eight splines of W (ghosts valid): (np, 41) property table."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        out = np.zeros((len(pos), 41))
+        self.L.orc_particle_props(C.byref(p), self._w5(W), spline_mode, len(pos), _ptr(pos), _ptr(out))
+        return out
+
+    def particle_stats(self, props: np.ndarray) -> np.ndarray:
+        """GetParticleStats on a property table: TKE, SijSij, SKEWu, SKEWw."""
+        props = np.ascontiguousarray(props, dtype=np.float64)
+        out = np.zeros(4)
+        self.L.orc_particle_stats(_ptr(props), len(props), _ptr(out))
+        return out
 
     # -- splines ---------------------------------------------------------------
     def spline1d(self, f: np.ndarray, periodic: int) -> np.ndarray:
@@ -207,6 +223,11 @@ class ReferenceRun:
         L.gkmref_time_steps.argtypes = [C.c_int, _dp, _dp]
         L.gkmref_flux.argtypes = [_dp] * 10 + [C.c_double] * 4 + [_dp]
         L.gkmref_weno.argtypes = [_dp, C.c_double, _dp, _dp]
+        L.gkmref_particle_table.argtypes = [_dp, C.POINTER(C.c_int)]
+        L.gkmref_particle_table.restype = C.c_int
+        L.gkmref_particle_stats.argtypes = [_dp]
+        L.gkmref_write_outputs.argtypes = [C.c_char_p]
+        L.gkmref_write_outputs.restype = C.c_int
         rc = L.gkmref_setup(icdir.encode(), cfl, 1 if with_particles else 0)
         if rc != 0:
             raise RuntimeError(f"gkmref_setup failed ({rc})")
@@ -245,6 +266,27 @@ class ReferenceRun:
         tags = np.zeros(max_count, dtype=np.int32)
         n = self.L.gkmref_get_particles(_ptr(pos), _ptr(U), tags.ctypes.data_as(C.POINTER(C.c_int)))
         return pos[:n], U[:n], tags[:n]
+
+    def particle_table(self, max_count: int):
+        """getParticleProp at the current positions: (count, 41) property table and tags."""
+        out = np.zeros((max_count, 41))
+        tags = np.zeros(max_count, dtype=np.int32)
+        n = self.L.gkmref_particle_table(_ptr(out), tags.ctypes.data_as(C.POINTER(C.c_int)))
+        return out[:n], tags[:n]
+
+    def particle_stats(self) -> np.ndarray:
+        """GetParticleStats after particle_table: part_TKE, part_SijSij, part_SKEWu, part_SKEWw."""
+        out = np.zeros(4)
+        self.L.gkmref_particle_stats(_ptr(out))
+        return out
+
+    def write_outputs(self, directory: str) -> None:
+        """The reference's own writeField / WriteReInit / writeParticleData into directory."""
+        for sub in ("Results/Field", "Results/Particles", "Results/Time", "InitialCondition"):
+            os.makedirs(os.path.join(directory, sub), exist_ok=True)
+        rc = self.L.gkmref_write_outputs(directory.encode())
+        if rc != 0:
+            raise RuntimeError(f"gkmref_write_outputs failed ({rc})")
 
     def time_steps(self, nsteps: int):
         te, tp = C.c_double(), C.c_double()

@@ -109,14 +109,18 @@ int gkmref_setup(const char *icdir, double cflnum, int with_particles)
 	int hs = 5 * 3 * nt_segx * nt_segz;
 	for (int b = 0; b < 12; b++)
 		S.halo[b] = new ptype[hs];
-	S.den = new ptype[Nt_seg];
-	S.u = new ptype[Nt_seg];
-	S.v = new ptype[Nt_seg];
-	S.w = new ptype[Nt_seg];
-	S.p = new ptype[Nt_seg];
-	S.lapU = new ptype[Nt_seg];
-	S.lapV = new ptype[Nt_seg];
-	S.lapW = new ptype[Nt_seg];
+	/* src/update.cpp:69-72 allocates these uninitialised; generateSplines writes
+	 * lapU/V/W only at interior nodes (src/update.cpp:1217-1228), so the ghost
+	 * nodes of the Laplacian splines keep the allocation's contents: zero pages
+	 * at the reference's sizes (fresh mmap'd blocks).  Zero them here. */
+	S.den = new ptype[Nt_seg]();
+	S.u = new ptype[Nt_seg]();
+	S.v = new ptype[Nt_seg]();
+	S.w = new ptype[Nt_seg]();
+	S.p = new ptype[Nt_seg]();
+	S.lapU = new ptype[Nt_seg]();
+	S.lapV = new ptype[Nt_seg]();
+	S.lapW = new ptype[Nt_seg]();
 	S.cflnum = cflnum;
 
 	/* src/update.cpp:94-120 */
@@ -307,6 +311,74 @@ void gkmref_time_steps(int nsteps, double *sec_eulerian, double *sec_particles)
 	}
 	*sec_eulerian = te;
 	*sec_particles = tp;
+}
+
+/* getParticleProp of every particle at its current position (the start of the
+ * next loop iteration) as the property table of include/gkm.h: per particle
+ * 41 values (DEN, gradD, U, gradU, gradV, gradW, P, gradP, hessP, lapU, lapV,
+ * lapW, gradLapU, gradLapV, gradLapW; gradients in (y, x, z) order); tags
+ * receives tagId.  Returns the particle count. */
+
+int gkmref_particle_table(double *out, int *tags)
+{
+	gkmref_particle_props();
+	for (int q = 0; q < ::count; q++)
+	{
+		const Particle &P = S.particles[q];
+		double *o = out + 41 * (size_t)q;
+		int m = 0;
+		o[m++] = P.DEN;
+		for (int a = 0; a < 3; a++) o[m++] = P.gradD[a];
+		for (int a = 0; a < 3; a++) o[m++] = P.U[a];
+		for (int a = 0; a < 3; a++) o[m++] = P.gradU[a];
+		for (int a = 0; a < 3; a++) o[m++] = P.gradV[a];
+		for (int a = 0; a < 3; a++) o[m++] = P.gradW[a];
+		o[m++] = P.P;
+		for (int a = 0; a < 3; a++) o[m++] = P.gradP[a];
+		for (int a = 0; a < 9; a++) o[m++] = P.hessP[a];
+		o[m++] = P.lapU;
+		o[m++] = P.lapV;
+		o[m++] = P.lapW;
+		for (int a = 0; a < 3; a++) o[m++] = P.gradLapU[a];
+		for (int a = 0; a < 3; a++) o[m++] = P.gradLapV[a];
+		for (int a = 0; a < 3; a++) o[m++] = P.gradLapW[a];
+		tags[q] = P.tagId;
+	}
+	return ::count;
+}
+
+/* GetParticleStats (src/update.cpp:1111-1162) after gkmref_particle_table */
+void gkmref_particle_stats(double *out4)
+{
+	GetParticleStats(S.particles, nullptr);
+	out4[0] = part_TKE;
+	out4[1] = part_SijSij;
+	out4[2] = part_SKEWu;
+	out4[3] = part_SKEWw;
+}
+
+/* The reference's own writers (writeField, WriteReInit, writeParticleData;
+ * src/update.cpp:1324-1422) on the current state, as at the top of a loop
+ * iteration, into <dir>/Results/{Field,Particles,Time} and
+ * <dir>/InitialCondition.  Returns 0 on success. */
+int gkmref_write_outputs(const char *dir)
+{
+	char old[4096];
+	if (!getcwd(old, sizeof(old)) || chdir(dir) != 0)
+		return -1;
+	UBspline_3d_d *sp[8];
+	generateSplines(S.W, sp, S.den, S.u, S.v, S.w, S.p, S.lapU, S.lapV, S.lapW);
+	writeField(S.den, S.u, S.v, S.w, S.p);
+	WriteReInit(S.W);
+	if (S.particles)
+	{
+		for (int q = 0; q < ::count; q++)
+			S.particles[q].getParticleProp(sp);
+		writeParticleData(S.particles);
+	}
+	for (int q = 0; q < 8; q++)
+		destroy_Bspline(sp[q]);
+	return chdir(old) == 0 ? 0 : -2;
 }
 
 /* direct calls into the reference numerics, for single-face checks */

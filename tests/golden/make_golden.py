@@ -11,6 +11,14 @@ Cases
   field_16 : 16^3, Mt 0.3, Re_lambda 30, cfl 0.5, 64 particles, 10 steps of Evolve's loop body
   field_12 : 12^3, Mt 0.6, Re_lambda 20, cfl 0.3, 24 particles, 5 steps
   faces    : single-face flux() and ApplyWENO() inputs/outputs (stencils cut from field_16 plus edge cases)
+  outputs_12 : the field_12 case at iteration 0 and after 3 steps: getParticleProp table,
+             GetParticleStats, and the files of writeField / writeParticleData (+ T file) /
+             WriteReInit as bytes
+  curve_32 : 32^3, Mt 0.3, Re_lambda 30, cfl 0.5, 200 steps: the PrintStats line every 10 steps
+  curve_64 : 64^3, Mt 0.3, Re_lambda 30, cfl 0.5, 100 steps (the 64^3 benchmark case), same
+
+    python tests/golden/make_golden.py --curves    (only the two curve cases; several minutes)
+    python tests/golden/make_golden.py --outputs   (only outputs_12)
 """
 from __future__ import annotations
 
@@ -51,6 +59,52 @@ def field_case(name: str, c: dict) -> dict:
     ref.particle_props()
     pos, U, tags = ref.particles(c["np"] * 2)
     out.update(pos_final=pos, U_final=U, tags=tags, stats_step0=stats0, stats_final=ref.stats())
+    return out
+
+
+CURVES = {
+    "curve_32": dict(n=32, Mt=0.3, Re=30.0, seed=4321, cfl=0.5, steps=200),
+    "curve_64": dict(n=64, Mt=0.3, Re=30.0, seed=1235, cfl=0.5, steps=100),
+}
+
+
+def curve_case(c: dict) -> dict:
+    """Long run of Evolve's loop body (no particles): dt of every step and the
+    PrintStats line at iterations 0, 10, 20, ... (gkmref_run)."""
+    d = O.tmpdir()
+    P, u, v, w, rho, p = ic.make_field(c["n"], c["Mt"], c["Re"], c["seed"])
+    ic.write_reference_inputs(d, P, u, v, w, rho, p, None)
+    ref = O.ReferenceRun(d, c["cfl"], False)
+    dts, stats = ref.run(c["steps"])
+    return dict(n=c["n"], cfl=c["cfl"], gam=P.gam, den0=P.den0, Mt=P.Mt, Re=P.Re, mu0=P.mu0, p0=P.p0, t0=P.t0,
+                seed=c["seed"], steps=c["steps"], dt=dts, stats=stats)
+
+
+def _read(path: str) -> np.ndarray:
+    with open(path, "rb") as f:
+        return np.frombuffer(f.read(), dtype=np.uint8)
+
+
+def outputs_case() -> dict:
+    c = CASES["field_12"]
+    d = O.tmpdir()
+    P, u, v, w, rho, p = ic.make_field(c["n"], c["Mt"], c["Re"], c["seed"])
+    ic.write_reference_inputs(d, P, u, v, w, rho, p, ic.make_particles(c["np"], c["seed"]))
+    ref = O.ReferenceRun(d, c["cfl"], True)
+    out = {}
+    for it in (0, 3):
+        if it:
+            ref.run(it)
+        props, tags = ref.particle_table(c["np"] * 2)
+        out[f"props_{it}"] = props
+        out[f"tags_{it}"] = tags
+        out[f"pstats_{it}"] = ref.particle_stats()
+        od = O.tmpdir()
+        ref.write_outputs(od)
+        out[f"field_{it}"] = _read(os.path.join(od, "Results", "Field", f"Field_0_{it}"))
+        out[f"particles_{it}"] = _read(os.path.join(od, "Results", "Particles", f"P_0_{it}"))
+        out[f"time_{it}"] = _read(os.path.join(od, "Results", "Time", f"T_{it}"))
+        out[f"reinit_{it}"] = _read(os.path.join(od, "InitialCondition", "Init000"))
     return out
 
 
@@ -108,6 +162,15 @@ def faces_case(field_W: np.ndarray, P, cfl: float) -> dict:
 
 def main() -> None:
     O.build(ref=True)
+    if "--outputs" in sys.argv:
+        np.savez_compressed(os.path.join(HERE, "outputs_12.npz"), **outputs_case())
+        print("outputs_12 written")
+        return
+    if "--curves" in sys.argv:
+        for name, c in CURVES.items():
+            np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **curve_case(c))
+            print(name, "written")
+        return
     results = {}
     for name, c in CASES.items():
         results[name] = field_case(name, c)

@@ -44,3 +44,22 @@ def test_seed_determinism():
     a = ic.make_field(8, 0.3, 30.0, seed=3)
     b = ic.make_field(8, 0.3, 30.0, seed=3)
     assert np.array_equal(a[1], b[1]) and a[0] == b[0]
+
+
+def test_device_state_generator_matches_numpy_recipe():
+    """make_state_device (torch, run here on the CPU) with NumPy's random draws
+    reproduces make_field + primitive_to_conserved to rounding."""
+    import torch  # noqa: F401
+
+    n = 32
+    rng = np.random.default_rng(7)
+    rand = [rng.random((n, n, n)) for _ in range(3)]
+    P, u, v, w, rho, p = ic.make_field(n, 0.4, 50.0, 7)
+    Wref = ic.primitive_to_conserved(P, u, v, w, rho, p)
+    P2, W2 = ic.make_state_device(n, 0.4, 50.0, 7, device="cpu", rand=rand)
+    W2 = W2.numpy()[:, 3:-3, 3:-3, 3:-3]
+    for q in range(5):
+        assert np.abs(W2[q] - Wref[q]).max() <= 1e-14 * np.abs(Wref[q]).max()
+    assert P2.mu0 == pytest.approx(P.mu0, rel=1e-13)
+    assert P2.t0 == pytest.approx(P.t0, rel=1e-13)
+    assert P2.Mt == pytest.approx(P.Mt, rel=1e-13)

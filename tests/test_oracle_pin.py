@@ -81,3 +81,23 @@ def test_halo_is_periodic_wrap(oracle, golden):
     V[:, :, -3:] = -1
     oracle.halo(p, V)
     assert np.array_equal(V, W)
+
+
+def _outputs_golden():
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "outputs_12.npz")
+    return dict(np.load(path))
+
+
+def test_particle_props_and_stats_bitexact(oracle, golden):
+    """getParticleProp (all eight splines) and GetParticleStats at iteration 0."""
+    g = golden["field_12"]
+    o = _outputs_golden()
+    P, W = _w0(g)
+    p = oracle.params(P, float(g["cfl"]))
+    oracle.halo(p, W)
+    pos = ic.particles_to_reference_order(g["particles_xyz"])
+    props = oracle.particle_props(p, W, pos)
+    order = np.argsort(o["tags_0"])
+    assert np.array_equal(props, o["props_0"][order])
+    assert np.array_equal(oracle.particle_stats(props), o["pstats_0"])
