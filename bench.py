@@ -308,7 +308,7 @@ def ours(args, rank: int, world: int, local_rank: int):
     s.set_stream(stream.cuda_stream)
     s.upload_state(W0)
     s.particles_upload(pos0)
-    sweep_cfg = s.autotune(args.autotune_reps)
+    sweep_cfg = s.autotune(args.autotune_reps) if args.autotune_reps > 0 else s.sweep_config()
     s.step_timed(args.warmup, True)
     torch.cuda.synchronize()
 
@@ -377,7 +377,7 @@ def ours(args, rank: int, world: int, local_rank: int):
         m.set_stream(stream.cuda_stream)
         m.upload_state(W0)
         m.particles_upload(pos0)
-        m_cfg = m.autotune(args.autotune_reps)
+        m_cfg = m.autotune(args.autotune_reps) if args.autotune_reps > 0 else m.sweep_config()
         m.step_timed(args.warmup, True)
         mph = m.step_timed(args.steps, True)
         Wm = m.download_state()
@@ -453,7 +453,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched ensemble forms")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer plug-point measurement")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="form of the main line")
-    ap.add_argument("--autotune-reps", type=int, default=2, help="timed launches per sweep shape")
+    ap.add_argument("--autotune-reps", type=int, default=2,
+                    help="timed launches per sweep shape; 0 keeps the default shapes (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
