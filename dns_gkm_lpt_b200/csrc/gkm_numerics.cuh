@@ -346,12 +346,18 @@ struct TimeCoefs {
     D gm1, gm2, gm3, gm4, gm5, p0, p1, p2, p3, p4, p5;
 };
 
-template <class D>
+// BGK time integrals over [0, dt] with e = exp(-dt/tau) (src/GKMflux.cpp:162-167,197-204).
+// EXPM1: 1 - e as -expm1(-dt/tau), exact where dt/tau is small (the mixed form,
+// whose flux runs in FP32 and gets these FP64 coefficients); otherwise the
+// reference's 1 - e.
+template <class D, bool EXPM1 = false>
 GKM_HD TimeCoefs<D> time_coefs(D tau, D dt)
 {
     TimeCoefs<D> c;
     D ex = exp_t<D>(-dt / tau);
-    D omx = D(1) - ex;
+    D omx;
+    if constexpr (EXPM1) omx = -expm1(-dt / tau);
+    else omx = D(1) - ex;
     D gm0 = dt - tau * omx;
     D igm0 = D(1) / gm0;
     c.gm1 = -omx * igm0;
@@ -409,7 +415,7 @@ GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[
 
     // collision time with the pressure-jump correction, src/GKMflux.cpp:156-157
     T ql = denl / laml, qr = denr / lamr;
-    const TimeCoefs<wide_t<T>> tc = time_coefs<wide_t<T>>(
+    const TimeCoefs<wide_t<T>> tc = time_coefs<wide_t<T>, (sizeof(T) < sizeof(wide_t<T>))>(
         wide_t<T>(tau0) + wide_t<T>(dt) * wide_t<T>(fabs(ql - qr) / fabs(ql + qr)), wide_t<T>(dt));
     const T gm1 = T(tc.gm1), gm2 = T(tc.gm2), gm3 = T(tc.gm3), gm4 = T(tc.gm4), gm5 = T(tc.gm5);
     const T p0 = T(tc.p0), p1 = T(tc.p1), p2 = T(tc.p2), p3 = T(tc.p3), p4 = T(tc.p4), p5 = T(tc.p5);
