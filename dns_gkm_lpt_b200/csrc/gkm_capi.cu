@@ -9,6 +9,7 @@
 #include "gkm.h"
 #include "gkm_handle.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -433,6 +434,9 @@ gkm_status gkm_destroy(gkm_handle* h)
     for (int c = 0; c < 5; c++) cudaFree(h->prop_coef[c]);
     cudaFree(h->lap_nodes);
     cudaFree(h->props);
+    for (cudaEvent_t e : h->pipe_ev) cudaEventDestroy(e);
+    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1]})
+        if (s) cudaStreamDestroy(s);
     cudaFree(h->partials);
     cudaFree(h->stats_out);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -656,10 +660,148 @@ gkm_status gkm_probe_fma_peak(int32_t device, double* fp64_tflops, double* fp32_
     return e == cudaSuccess ? GKM_OK : GKM_ERR_CUDA;
 }
 
+namespace {
+
+// copy engines can read and write these asynchronously: pinned host or device memory
+bool async_capable(const double* p)
+{
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost || at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// The plug point evolve(W, dt) as a pipeline over chunks of y-planes: the host -> device copy of
+// chunk c+1, the x/y/z sweeps of chunk c and the device -> host copy of chunk c-1 overlap.  A
+// chunk's sweeps need the input planes within 3 of it (y stencil) with their ghosts; the
+// copy-in stream wraps each chunk's ghosts as it arrives (the periodic y-ghost planes come from
+// the last three interior planes, copied first, and from the first chunk), so chunk c waits for
+// the copy-in of chunk c+1.  Each chunk writes only its own planes of the accumulator, so two
+// compute streams run consecutive chunks concurrently.  Results equal the one-shot path.
+gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
+{
+    const FieldConst& fc = h->fc;
+    const int n = fc.n;
+    const size_t plane = (size_t)fc.nt * fc.nt, nt3 = (size_t)fc.nt3;
+    int C = ((n / 8 + 15) / 16) * 16;   // a multiple of every window height, about n/8
+    if (C < 16) C = 16;
+    const int K = (n + C - 1) / C;
+    if (!h->pipe_in) {
+        for (cudaStream_t* s : {&h->pipe_in, &h->pipe_out, &h->pipe_comp[0], &h->pipe_comp[1]})
+            CK(h, cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+    }
+    const size_t nev = 2 * (size_t)K + 2;
+    while (h->pipe_ev.size() < nev) {
+        cudaEvent_t e;
+        CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->pipe_ev.push_back(e);
+    }
+    cudaEvent_t ev_start = h->pipe_ev[0], ev_done_out = h->pipe_ev[1];
+    cudaEvent_t* ev_in = &h->pipe_ev[2];
+    cudaEvent_t* ev_out = &h->pipe_ev[2 + K];
+    double* Wd = h->buf[h->parity];
+    double* A = h->buf[h->parity ^ 1];
+    DevClock* ck = h->clock;
+    const bool mixed = h->cfg.precision == GKM_PREC_MIXED;
+
+    // the clock: this step's dt, the next wave slot cleared (the z sweeps reduce into it), status
+    CK(h, cudaMemcpyAsync(&ck->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemsetAsync(&ck->wave[h->parity ^ 1], 0, sizeof(unsigned long long), h->stream));
+    CK(h, cudaMemsetAsync(&ck->status, 0, sizeof(int), h->stream));
+    CK(h, cudaEventRecord(ev_start, h->stream));
+    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1]})
+        CK(h, cudaStreamWaitEvent(s, ev_start, 0));
+
+    auto copy_in = [&](int J0, int J1) -> cudaError_t {
+        for (int q = 0; q < 5; q++) {
+            const size_t off = (size_t)q * nt3 + (size_t)J0 * plane;
+            cudaError_t e = cudaMemcpyAsync(Wd + off, W[q] + (size_t)J0 * plane, sizeof(double) * (J1 - J0) * plane,
+                                            cudaMemcpyDefault, h->pipe_in);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    auto copy_out = [&](int J0, int J1, cudaStream_t s) -> cudaError_t {
+        for (int q = 0; q < 5; q++) {
+            const size_t off = (size_t)q * nt3 + (size_t)J0 * plane;
+            cudaError_t e = cudaMemcpyAsync(W[q] + (size_t)J0 * plane, A + off, sizeof(double) * (J1 - J0) * plane,
+                                            cudaMemcpyDefault, s);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+
+    // copy-in stream: the last three interior planes first, then the chunks, each with its ghosts
+    CK(h, copy_in(n, n + 3));
+    for (int c = 0; c < K; c++) {
+        const int J0 = 3 + c * C, J1 = 3 + std::min((c + 1) * C, n);
+        const int J1c = (J0 < n) ? std::min(J1, n) : J1;   // planes n..n+2 are already in
+        if (J1c > J0) CK(h, copy_in(J0, J1c));
+        if (c == 0) {
+            CK(h, gkm::launch_halo_planes(Wd, fc, 0, 3, h->pipe_in));
+            CK(h, gkm::launch_halo_planes(Wd, fc, n + 3, n + 6, h->pipe_in));
+            h->launches += 2;
+        }
+        CK(h, gkm::launch_halo_planes(Wd, fc, J0, J1, h->pipe_in));
+        h->launches += 1;
+        CK(h, cudaEventRecord(ev_in[c], h->pipe_in));
+    }
+
+    // compute: chunk c on compute stream c % 2, after the copy-in of chunk c+1
+    gkm::SweepArgs a{};
+    a.W = Wd;
+    a.A = A;
+    a.fc = fc;
+    a.clock = ck;
+    a.parity = h->parity;
+    a.dt_fixed_mode = 1;
+    a.dt_fixed = dt;
+    a.skip_clock_init = 1;
+    for (int c = 0; c < K; c++) {
+        cudaStream_t s = h->pipe_comp[c % 2];
+        CK(h, cudaStreamWaitEvent(s, ev_in[std::min(c + 1, K - 1)], 0));
+        const int j0 = c * C, j1 = std::min((c + 1) * C, n);
+        for (int d = 0; d < 3; d++) {
+            gkm::SweepArgs ad = a;
+            ad.seg_len = (d == 1) ? C : h->sweep[d].seg_len;
+            const int v = h->sweep[d].variant;
+            CK(h, mixed ? gkm::launch_sweep_mixed_rows(d, v, ad, j0, j1, s) : gkm::launch_sweep_rows(d, v, ad, j0, j1, s));
+        }
+        CK(h, gkm::launch_halo_planes(A, fc, 3 + j0, 3 + j1, s));
+        h->launches += 4;
+        CK(h, cudaEventRecord(ev_out[c], s));
+        CK(h, cudaStreamWaitEvent(h->pipe_out, ev_out[c], 0));
+        CK(h, copy_out(3 + j0, 3 + j1, h->pipe_out));
+    }
+    CK(h, cudaEventRecord(ev_done_out, h->pipe_out));
+
+    // the y-ghost planes of the new state, the clock, the last copies
+    for (int c = 0; c < K; c++) CK(h, cudaStreamWaitEvent(h->stream, ev_out[c], 0));
+    CK(h, gkm::launch_halo_planes(A, fc, 0, 3, h->stream));
+    CK(h, gkm::launch_halo_planes(A, fc, n + 3, n + 6, h->stream));
+    CK(h, gkm::launch_clock_finish(ck, dt, h->stream));
+    h->launches += 3;
+    CK(h, copy_out(0, 3, h->stream));
+    CK(h, copy_out(n + 3, n + 6, h->stream));
+    CK(h, cudaStreamWaitEvent(h->stream, ev_done_out, 0));
+    h->parity ^= 1;
+    h->state_loaded = true;
+    h->splines_valid = false;
+    DevClock c;
+    return read_clock(h, &c);
+}
+
+}  // namespace
+
 gkm_status gkm_evolve(gkm_handle* h, double* const W[5], double dt)
 {
     if (!h || !W) return GKM_ERR_ARG;
     if (!(dt > 0.0)) return fail(h, GKM_ERR_ARG, "dt must be > 0");
+    bool pipelined = true;
+    for (int q = 0; q < 5; q++) pipelined = pipelined && W[q] && async_capable(W[q]);
+    if (pipelined) return evolve_pipelined(h, W, dt);
     gkm_status s = gkm_upload_state(h, (const double* const*)W);
     if (s != GKM_OK) return s;
     const int mode = h->dt_fixed_mode;

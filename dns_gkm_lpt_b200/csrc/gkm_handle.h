@@ -6,6 +6,7 @@
 #include "gkm_internal.h"
 
 #include <string>
+#include <vector>
 
 struct gkm_ensemble;
 
@@ -43,6 +44,10 @@ struct gkm_handle {
     int64_t graph_np[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};
     int64_t graph_kernels[3][2] = {{0, 0}, {0, 0}, {0, 0}};
     int64_t launches = 0;    // kernels launched (graph replays add the kernels they hold)
+    // plug-point pipeline (gkm_evolve with pinned or device buffers): copy-in, copy-out and
+    // two compute streams, and per-chunk events, created on first use
+    cudaStream_t pipe_in = nullptr, pipe_out = nullptr, pipe_comp[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> pipe_ev;
     std::string err;
     gkm_ensemble* owner = nullptr;   // set while the handle is a member of an ensemble
 };

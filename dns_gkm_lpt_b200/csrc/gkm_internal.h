@@ -78,11 +78,23 @@ struct SweepArgs {
     int dt_fixed_mode;              // 1: use dt_fixed instead of cfl dx / max(|u|+c)
     double dt_fixed;
     int seg_len;                    // faces per CTA along the normal
+    int tile_a0;                    // first window row (x, z sweeps) of a launch over part of the j range
+    int seg0;                       // first segment (y sweep) of such a launch
+    int skip_clock_init;            // 1: the clock's dt and next wave slot were set before the launch
 };
 
 // kernel launchers (sweep.cu); sweep_prepare sets the sweep kernels' shared-memory limit once
 cudaError_t sweep_prepare();
 cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s);
+// The sweep of direction dir restricted to the interior y-planes [j0, j1): window rows (x, z
+// sweeps) or normal segments (y sweep) covering them; j0 must be a multiple of the window height
+// (x, z) or of a.seg_len (y).  The cells updated are exactly those of planes [j0, j1).
+cudaError_t launch_sweep_rows(int dir, int variant, SweepArgs a, int j0, int j1, cudaStream_t s);
+cudaError_t launch_sweep_mixed_rows(int dir, int variant, SweepArgs a, int j0, int j1, cudaStream_t s);
+// Ghost cells of the ghost-layout y-planes [J0, J1) (0 <= J0 < J1 <= nt) from their periodic images
+cudaError_t launch_halo_planes(double* W, const FieldConst& fc, int J0, int J1, cudaStream_t s);
+// the clock update that closes a step with a given dt: t += dt, iter += 1
+cudaError_t launch_clock_finish(DevClock* clock, double dt, cudaStream_t s);
 // the same sweeps with the reconstruction and the flux in single precision (sweep_mixed.cu)
 cudaError_t launch_sweep_mixed(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s);
 cudaError_t sweep_mixed_prepare();

@@ -36,6 +36,34 @@ __global__ void halo_kernel(double* __restrict__ W, FieldConst fc, DevClock* clo
         halo_cell(W, fc, g);
 }
 
+// ghost cells of the y-planes [J0, J1): every cell with a coordinate outside the interior takes the
+// value of its periodic image, which is interior in all three coordinates
+__global__ void halo_planes_kernel(double* __restrict__ W, FieldConst fc, int J0, int J1)
+{
+    const int n = fc.n, nt = fc.nt;
+    const long long nt2 = (long long)nt * nt, nt3 = fc.nt3;
+    const long long total = (long long)(J1 - J0) * nt2;
+    auto wrap = [n](int x) { return x < 3 ? x + n : (x >= n + 3 ? x - n : x); };
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int j = J0 + (int)(e / nt2);
+        const long long rem = e - (long long)(j - J0) * nt2;
+        const int i = (int)(rem / nt), k = (int)(rem - (long long)i * nt);
+        const int wj = wrap(j), wi = wrap(i), wk = wrap(k);
+        if (wj == j && wi == i && wk == k) continue;   // interior cell
+        const long long dst = ((long long)j * nt + i) * nt + k;
+        const long long src = ((long long)wj * nt + wi) * nt + wk;
+#pragma unroll
+        for (int q = 0; q < 5; q++) W[q * nt3 + dst] = W[q * nt3 + src];
+    }
+}
+
+__global__ void clock_finish_kernel(DevClock* clock, double dt)
+{
+    clock->t += dt;   // src/update.cpp:167-168 with the next step's dt (the given one)
+    clock->iter += 1;
+}
+
 __global__ void wave_reduce_kernel(const double* __restrict__ W, FieldConst fc, DevClock* clock, int slot)
 {
     __shared__ double red[32];
@@ -197,6 +225,28 @@ cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cud
     if (dir == 0) return launch_one<0, SweepTile64a>(a, nseg, s);
     if (dir == 1) return launch_one<1, SweepTile64a>(a, nseg, s);
     return launch_one<2, SweepTile64a>(a, nseg, s);
+}
+
+cudaError_t launch_sweep_rows(int dir, int variant, SweepArgs a, int j0, int j1, cudaStream_t s)
+{
+    if (variant == 1) return launch_sweep_rows_t<double, SweepTile64b>(dir, a, j0, j1, s);
+    return launch_sweep_rows_t<double, SweepTile64a>(dir, a, j0, j1, s);
+}
+
+cudaError_t launch_halo_planes(double* W, const FieldConst& fc, int J0, int J1, cudaStream_t s)
+{
+    if (J0 < 0 || J1 > fc.nt || J0 >= J1) return cudaErrorInvalidValue;
+    const long long total = (long long)(J1 - J0) * fc.nt * fc.nt;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    halo_planes_kernel<<<(unsigned)blocks, 256, 0, s>>>(W, fc, J0, J1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_clock_finish(DevClock* clock, double dt, cudaStream_t s)
+{
+    clock_finish_kernel<<<1, 1, 0, s>>>(clock, dt);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_halo(double* W, const FieldConst& fc, DevClock* clock, int finish_step, int slot,

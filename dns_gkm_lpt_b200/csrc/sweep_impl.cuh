@@ -195,7 +195,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     const T eps_T = kMixed ? T(fc.eps_T) : T(kWenoEps);
     const double* __restrict__ W = a.W;
 
-    if (DIR == 0 && bx == 0 && by == 0 && bz == 0 && tid == 0) {
+    if (DIR == 0 && bx == 0 && by == 0 && bz == 0 && tid == 0 && !a.skip_clock_init) {
         a.clock->wave[a.parity ^ 1] = 0ull;   // the z sweep of this step reduces into it
         a.clock->dt = dt;
     }
@@ -350,7 +350,7 @@ template <int DIR, class T, class Tile>
 __global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    sweep_block<DIR, T, Tile>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+    sweep_block<DIR, T, Tile>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z + a.seg0, smem_raw);
 }
 
 // Persistent form for an ensemble: a fixed grid of CTAs walks the flattened
@@ -372,6 +372,9 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
         const int bz = (int)(local % nseg);
         const long long t = local / nseg;
         SweepArgs a;
+        a.tile_a0 = 0;
+        a.seg0 = 0;
+        a.skip_clock_init = 0;
         a.W = md.buf[parity];
         a.A = md.buf[parity ^ 1];
         a.fc = md.fc;
@@ -383,6 +386,29 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
         sweep_block<DIR, T, Tile>(a, (int)(t % tb), (int)(t / tb), bz, smem_raw);
         __syncthreads();   // the next item reuses the shared-memory ring
     }
+}
+
+template <class T, class Tile>
+cudaError_t launch_sweep_rows_t(int dir, SweepArgs a, int j0, int j1, cudaStream_t s)
+{
+    const int n = a.fc.n;
+    if (j0 < 0 || j1 > n || j0 >= j1) return cudaErrorInvalidValue;
+    const int gb = (n + Tile::TB - 1) / Tile::TB;
+    const size_t smem = sweep_detail::sweep_smem_bytes<T, Tile>();
+    const dim3 block(Tile::TB, Tile::TA);
+    if (dir == 1) {
+        if (j0 % a.seg_len) return cudaErrorInvalidValue;
+        a.seg0 = j0 / a.seg_len;
+        const dim3 grid(gb, (n + Tile::TA - 1) / Tile::TA, (j1 + a.seg_len - 1) / a.seg_len - a.seg0);
+        sweep_kernel<1, T, Tile><<<grid, block, smem, s>>>(a);
+        return cudaGetLastError();
+    }
+    if (j0 % Tile::TA) return cudaErrorInvalidValue;
+    a.tile_a0 = j0 / Tile::TA;
+    const dim3 grid(gb, (j1 + Tile::TA - 1) / Tile::TA - a.tile_a0, (n + a.seg_len - 1) / a.seg_len);
+    if (dir == 0) sweep_kernel<0, T, Tile><<<grid, block, smem, s>>>(a);
+    else sweep_kernel<2, T, Tile><<<grid, block, smem, s>>>(a);
+    return cudaGetLastError();
 }
 
 template <class T, class Tile>

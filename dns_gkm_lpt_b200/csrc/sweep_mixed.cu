@@ -47,6 +47,12 @@ cudaError_t launch_ensemble_sweep32(int dir, int variant, const MemberDev* mem, 
     return launch_ensemble_sweep_t<float, SweepTile32a>(dir, mem, off, nm, parity, seg_len, s);
 }
 
+cudaError_t launch_sweep_mixed_rows(int dir, int variant, SweepArgs a, int j0, int j1, cudaStream_t s)
+{
+    (void)variant;
+    return launch_sweep_rows_t<float, SweepTile32a>(dir, a, j0, j1, s);
+}
+
 cudaError_t launch_sweep_mixed(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s)
 {
     (void)variant;   // one window for the single-precision sweeps

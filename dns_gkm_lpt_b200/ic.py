@@ -59,6 +59,8 @@ def _kfft(n: int) -> np.ndarray:
 def make_field(n: int, Mt: float, Re: float, seed: int, k0: float = 4.0, kcmin: float = 1.0,
                kcmax: float = 8.0, gam: float = 1.4, rho0: float = 1.0, T0: float = 300.0):
     """Return (params, u, v, w, rho, p) with u, v, w, rho, p shaped (y, x, z)."""
+    if n % 2:
+        raise ValueError("n must be even (the wavenumber layout of init_DNS.m)")
     rng = np.random.default_rng(seed)
     Np = float(n) ** 3
     A = np.sqrt(2.0 / np.pi) * (16.0 / 3.0) * Mt ** 2 / k0 ** 5
@@ -193,6 +195,8 @@ def make_state_device(n: int, Mt: float, Re: float, seed: int, device="cuda", k0
     """
     import torch
 
+    if n % 2:
+        raise ValueError("n must be even (the wavenumber layout of init_DNS.m)")
     dev = torch.device(device)
     f64 = torch.float64
     Np = float(n) ** 3

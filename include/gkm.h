@@ -134,7 +134,10 @@ gkm_status gkm_evolve_eulerian(gkm_handle* h, int32_t nsteps);
 /* The reference's GPU plug point, void evolve(ptype *W[5], DevAlloc *dev,
  * ptype dt) (src/GPUupdate.h:33, src/GPUupdate.cu:79-219): copy W in, take
  * one Eulerian step with the given dt, copy W out.  Synchronous.  The output
- * ghosts are already wrapped. */
+ * ghosts are already wrapped.  With pinned (cudaHostAlloc / cudaHostRegister)
+ * or device W the step runs as a pipeline over chunks of y-planes, so the
+ * copies in and out overlap the sweeps; pageable W takes one copy in, the
+ * step, one copy out.  Both give the same result. */
 gkm_status gkm_evolve(gkm_handle* h, double* const W[5], double dt);
 
 /* nsteps of the body of Evolve's loop (src/update.cpp:124-170): Eulerian
