@@ -139,9 +139,78 @@ cudaError_t enqueue_eulerian(gkm_handle* h)
 
 cudaError_t enqueue_splines(gkm_handle* h, const double* W)
 {
+    if (h->d_self && (W == h->buf[0] || W == h->buf[1])) {
+        gkm::EnsembleWork w{};
+        w.line0 = h->d_self_off;
+        w.line1 = h->d_self_off + 2;
+        w.warp2 = h->d_self_off + 4;
+        h->launches += 3;
+        return gkm::launch_ensemble_splines(h->d_self, w, h->self_totals, 1, W == h->buf[0] ? 0 : 1, h->stream);
+    }
     h->launches += kSplinePasses;
     return gkm::launch_spline_build(W, h->fc, h->grid, device_tables(h), h->coef[0], h->coef[1], h->coef[2],
                                     h->scratch, h->stream);
+}
+
+// Set up the component-batched spline build where it pays: when one component's N^2 lines
+// leave most of the GPU's thread slots (148 SMs x 2048) idle, and the device has room for two
+// more scratch arrays.  Larger grids fill the GPU per component already.
+cudaError_t setup_batched_splines(gkm_handle* h)
+{
+    const long long N = h->grid.npts, M = N + h->grid.pad;
+    if (3 * N * N > 2LL * 148 * 2048) return cudaSuccess;
+    const size_t scratch_bytes = sizeof(double) * (size_t)(M * M * N);
+    size_t free_b = 0, total_b = 0;
+    cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess) return e;
+    if (free_b < 2 * scratch_bytes + ((size_t)8 << 30)) return cudaSuccess;   // keep 8 GB for the caller
+    for (int k = 0; k < 2; k++) {
+        e = cudaMalloc(&h->scratch_extra[k], scratch_bytes);
+        if (e != cudaSuccess) return e;
+    }
+    gkm::MemberDev md;
+    std::memset(&md, 0, sizeof(md));
+    md.buf[0] = h->buf[0];
+    md.buf[1] = h->buf[1];
+    md.clock = h->clock;
+    md.fc = h->fc;
+    md.grid = h->grid;
+    md.tb = device_tables(h);
+    for (int c = 0; c < 3; c++) md.coef[c] = h->coef[c];
+    md.scratch[0] = h->scratch;
+    md.scratch[1] = h->scratch_extra[0];
+    md.scratch[2] = h->scratch_extra[1];
+    const long long off[6] = {0, 3 * N * N, 0, 3 * M * N, 0, 3 * ((M * M + 31) / 32)};
+    h->self_totals[0] = off[1];
+    h->self_totals[1] = off[3];
+    h->self_totals[2] = off[5];
+    e = cudaMalloc(&h->d_self, sizeof(md));
+    if (e == cudaSuccess) e = cudaMalloc(&h->d_self_off, sizeof(off));
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_self, &md, sizeof(md), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_self_off, off, sizeof(off), cudaMemcpyHostToDevice);
+    return e;
+}
+
+gkm::ParticleArrays arrays_of(double* const a[6])
+{
+    return gkm::ParticleArrays{{a[0], a[1], a[2], a[3], a[4], a[5]}};
+}
+
+// order the particles by spline-cell blocks (into the sorted copy), then Heun from the sorted
+// copy back into the particle arrays with the dt of the last Eulerian step
+cudaError_t enqueue_advect(gkm_handle* h)
+{
+    if (h->np <= 0) return cudaSuccess;
+    int nl = 0;
+    cudaError_t e = gkm::launch_particle_sort(h->grid, h->np, arrays_of(h->P), arrays_of(h->P_sorted), h->tag,
+                                              h->tag_sorted, h->sort_keys, h->sort_counts, h->sort_temp, &nl,
+                                              h->stream);
+    h->launches += nl + 1;
+    if (e != cudaSuccess) return e;
+    const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+    h->launches += 1;
+    return gkm::launch_particles_heun(c, h->grid, h->clock, h->np, arrays_of(h->P_sorted), arrays_of(h->P),
+                                      h->tag_sorted, h->tag, h->stream);
 }
 
 // splines of the state W and Heun advection with the dt of the last Eulerian step
@@ -150,10 +219,7 @@ cudaError_t enqueue_particles(gkm_handle* h, const double* W)
     if (h->np <= 0) return cudaSuccess;
     cudaError_t e = enqueue_splines(h, W);
     if (e != cudaSuccess) return e;
-    const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
-    h->launches += 1;
-    return gkm::launch_particles_heun(c, h->grid, h->clock, h->np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4],
-                                      h->P[5], h->stream);
+    return enqueue_advect(h);
 }
 
 // the body of Evolve's loop: Eulerian step, splines of the new state, particles
@@ -233,6 +299,18 @@ gkm_status ensure_splines(gkm_handle* h)
     return GKM_OK;
 }
 
+// upload index of the particle in each device slot (the arrays are kept in spline-cell order)
+gkm_status host_tags(gkm_handle* h, std::vector<long long>& tags)
+{
+    tags.resize((size_t)h->np);
+    if (h->np == 0) return GKM_OK;
+    CK(h, cudaMemcpyAsync(tags.data(), h->tag, sizeof(long long) * (size_t)h->np, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    for (long long t : tags)
+        if (t < 0 || t >= h->np) return fail(h, GKM_ERR_STATE, "particle tags corrupted");
+    return GKM_OK;
+}
+
 // the five further splines of the reference's 8-field generateSplines
 // (src/update.cpp:1200-1233) and getParticleProp for every particle
 // (src/ParticleTrack.cpp:99-113) into h->props; allocates on first use
@@ -276,9 +354,12 @@ gkm_status gkm_host_props(gkm_handle* h, double* out)
     std::vector<double> tmp((size_t)gkm::kPropCount * (size_t)h->np);
     CK(h, cudaMemcpyAsync(tmp.data(), h->props, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
+    std::vector<long long> tags;
+    s = host_tags(h, tags);
+    if (s != GKM_OK) return s;
     const size_t np = (size_t)h->np;
     for (size_t p = 0; p < np; p++)
-        for (int q = 0; q < gkm::kPropCount; q++) out[p * gkm::kPropCount + q] = tmp[(size_t)q * np + p];
+        for (int q = 0; q < gkm::kPropCount; q++) out[(size_t)tags[p] * gkm::kPropCount + q] = tmp[(size_t)q * np + p];
     return GKM_OK;
 }
 
@@ -403,11 +484,20 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     if (e != cudaSuccess) return bail(e, "cudaMalloc(spline scratch)");
     // particles
     h->cap = cfg->max_particles;
-    if (h->cap > 0)
+    if (h->cap > 0) {
         for (int c = 0; c < 6; c++) {
             e = cudaMalloc(&h->P[c], sizeof(double) * (size_t)h->cap);
+            if (e == cudaSuccess) e = cudaMalloc(&h->P_sorted[c], sizeof(double) * (size_t)h->cap);
             if (e != cudaSuccess) return bail(e, "cudaMalloc(particles)");
         }
+        const long long nb = (h->grid.npts + 7) / 8, nkeys = nb * nb * nb;
+        e = cudaMalloc(&h->tag, sizeof(long long) * (size_t)h->cap);
+        if (e == cudaSuccess) e = cudaMalloc(&h->tag_sorted, sizeof(long long) * (size_t)h->cap);
+        if (e == cudaSuccess) e = cudaMalloc(&h->sort_keys, sizeof(unsigned) * (size_t)h->cap);
+        if (e == cudaSuccess) e = cudaMalloc(&h->sort_counts, sizeof(unsigned) * (size_t)nkeys);
+        if (e == cudaSuccess) e = cudaMalloc(&h->sort_temp, sizeof(unsigned) * (size_t)gkm::scan_temp_size(nkeys));
+        if (e != cudaSuccess) return bail(e, "cudaMalloc(particle ordering)");
+    }
     e = cudaMalloc(&h->partials, sizeof(gkm::StatsPartial) * kStatsBlocks);
     if (e != cudaSuccess) return bail(e, "cudaMalloc(stats)");
     e = cudaMalloc(&h->stats_out, sizeof(double) * 32);
@@ -415,6 +505,8 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     e = gkm::sweep_prepare();
     if (e == cudaSuccess) e = gkm::sweep_mixed_prepare();
     if (e != cudaSuccess) return bail(e, "sweep_prepare");
+    e = setup_batched_splines(h);
+    if (e != cudaSuccess) return bail(e, "batched spline build");
     *out = h;
     return GKM_OK;
 }
@@ -430,7 +522,18 @@ gkm_status gkm_destroy(gkm_handle* h)
     cudaFree(h->tables);
     for (int c = 0; c < 3; c++) cudaFree(h->coef[c]);
     cudaFree(h->scratch);
-    for (int c = 0; c < 6; c++) cudaFree(h->P[c]);
+    for (int k = 0; k < 2; k++) cudaFree(h->scratch_extra[k]);
+    cudaFree(h->d_self);
+    cudaFree(h->d_self_off);
+    for (int c = 0; c < 6; c++) {
+        cudaFree(h->P[c]);
+        cudaFree(h->P_sorted[c]);
+    }
+    cudaFree(h->tag);
+    cudaFree(h->tag_sorted);
+    cudaFree(h->sort_keys);
+    cudaFree(h->sort_counts);
+    cudaFree(h->sort_temp);
     for (int c = 0; c < 5; c++) cudaFree(h->prop_coef[c]);
     cudaFree(h->lap_nodes);
     cudaFree(h->props);
@@ -542,12 +645,7 @@ gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles,
         const bool parts = with_particles && h->np > 0;
         if (e == cudaSuccess && parts) e = enqueue_splines(h, h->buf[h->parity]);
         if (e == cudaSuccess) e = cudaEventRecord(ev[5], h->stream);
-        if (e == cudaSuccess && parts) {
-            const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
-            e = gkm::launch_particles_heun(c, h->grid, h->clock, h->np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4],
-                                           h->P[5], h->stream);
-            h->launches += 1;
-        }
+        if (e == cudaSuccess && parts) e = enqueue_advect(h);
         if (e == cudaSuccess) e = cudaEventRecord(ev[6], h->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(ev[6]);
         if (e != cudaSuccess) {
@@ -847,6 +945,12 @@ gkm_status gkm_particles_upload(gkm_handle* h, int64_t np, const double* pos, co
         CK(h, cudaMemcpyAsync(h->P[c], tmp.data(), sizeof(double) * (size_t)np, cudaMemcpyHostToDevice, h->stream));
         CK(h, cudaStreamSynchronize(h->stream));
     }
+    if (np > 0) {   // tags: the upload order, restored by every download
+        std::vector<long long> tags((size_t)np);
+        for (int64_t p = 0; p < np; p++) tags[(size_t)p] = p;
+        CK(h, cudaMemcpyAsync(h->tag, tags.data(), sizeof(long long) * (size_t)np, cudaMemcpyHostToDevice, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
     h->np = np;
     if (!U && np > 0) {
         if (!h->state_loaded) return fail(h, GKM_ERR_STATE, "U == NULL needs an uploaded state");
@@ -864,12 +968,15 @@ gkm_status gkm_particles_download(gkm_handle* h, double* pos, double* U)
 {
     if (!h) return GKM_ERR_ARG;
     std::vector<double> tmp((size_t)h->np);
+    std::vector<long long> tags;
+    gkm_status s = host_tags(h, tags);
+    if (s != GKM_OK) return s;
     for (int c = 0; c < 6; c++) {
         double* dst = c < 3 ? pos : U;
         if (!dst) continue;
         CK(h, cudaMemcpyAsync(tmp.data(), h->P[c], sizeof(double) * (size_t)h->np, cudaMemcpyDeviceToHost, h->stream));
         CK(h, cudaStreamSynchronize(h->stream));
-        for (int64_t p = 0; p < h->np; p++) dst[3 * p + (c % 3)] = tmp[(size_t)p];
+        for (int64_t p = 0; p < h->np; p++) dst[3 * tags[(size_t)p] + (c % 3)] = tmp[(size_t)p];
     }
     DevClock c;
     return read_clock(h, &c);

@@ -26,7 +26,7 @@ enum OffsetSet { kItemX = 0, kItemY, kItemZ, kGhost, kLine0, kLine1, kWarp2, kPa
 
 struct gkm_ensemble {
     std::vector<gkm_handle*> mem;
-    std::vector<double*> extra_scratch;   // two more spline scratch arrays per member
+    std::vector<double*> extra_scratch;   // two more spline scratch arrays per member (unless it has its own)
     bool mixed = false;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -112,8 +112,8 @@ gkm_status refresh(gkm_ensemble* E, bool need_state)
         md.tb = gkm::SplineTables{h->tables, h->tables + N1, h->tables + 2 * N1, h->denom};
         for (int c = 0; c < 3; c++) md.coef[c] = h->coef[c];
         md.scratch[0] = h->scratch;
-        md.scratch[1] = E->extra_scratch[2 * (size_t)m];
-        md.scratch[2] = E->extra_scratch[2 * (size_t)m + 1];
+        md.scratch[1] = h->scratch_extra[0] ? h->scratch_extra[0] : E->extra_scratch[2 * (size_t)m];
+        md.scratch[2] = h->scratch_extra[1] ? h->scratch_extra[1] : E->extra_scratch[2 * (size_t)m + 1];
         for (int c = 0; c < 6; c++) md.P[c] = h->P[c];
         md.np = h->np;
         const long long N = h->grid.npts, M = N + h->grid.pad;
@@ -235,9 +235,11 @@ gkm_status gkm_ensemble_create(const gkm_config* members, int32_t n_members, gkm
         E->mem.push_back(h);
         const long long M = h->grid.npts + h->grid.pad, N = h->grid.npts;
         for (int k = 0; k < 2; k++) {
-            double* p = nullptr;
-            e = cudaMalloc(&p, sizeof(double) * (size_t)(M * M * N));
-            if (e != cudaSuccess) return bail(ecuda(E, e, "cudaMalloc(spline scratch)"));
+            double* p = nullptr;   // the member's own second and third scratch when it has them
+            if (!h->scratch_extra[k]) {
+                e = cudaMalloc(&p, sizeof(double) * (size_t)(M * M * N));
+                if (e != cudaSuccess) return bail(ecuda(E, e, "cudaMalloc(spline scratch)"));
+            }
             E->extra_scratch.push_back(p);
         }
         if (h->fc.n > max_n) max_n = h->fc.n;

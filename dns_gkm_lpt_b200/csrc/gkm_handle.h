@@ -32,9 +32,23 @@ struct gkm_handle {
     double denom = 0.0;
     double* coef[3] = {nullptr, nullptr, nullptr};
     double* scratch = nullptr;
+    // the three velocity splines built together (one launch per pass for all three components):
+    // two more scratch arrays and a one-member descriptor for the ensemble spline kernels;
+    // left out when the device lacks the memory (large grids), then one component at a time
+    double* scratch_extra[2] = {nullptr, nullptr};
+    gkm::MemberDev* d_self = nullptr;
+    long long* d_self_off = nullptr;   // line0 | line1 | warp2 prefix offsets, 2 each
+    long long self_totals[3] = {0, 0, 0};
     bool splines_valid = false;
     int64_t np = 0, cap = 0;
     double* P[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // y, x, z, u, v, w
+    // particle ordering: the sorted copy, upload indices (tags) of both, keys and bucket counts
+    double* P_sorted[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    long long* tag = nullptr;          // upload index of the particle in each slot of P
+    long long* tag_sorted = nullptr;
+    unsigned* sort_keys = nullptr;
+    unsigned* sort_counts = nullptr;
+    unsigned* sort_temp = nullptr;
     double* prop_coef[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // rho, p, lap u, lap v, lap w
     double* lap_nodes = nullptr;     // nt^3 Laplacian node values (one velocity component at a time)
     double* props = nullptr;         // [kPropCount][cap] particle properties

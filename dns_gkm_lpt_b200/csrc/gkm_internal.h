@@ -139,9 +139,18 @@ cudaError_t launch_spline_component(const double* W, const FieldConst& fc, const
 cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np,
                                   const double* py, const double* px, const double* pz,
                                   double* Uu, double* Uv, double* Uw, cudaStream_t s);
+struct ParticleArrays {   // y, x, z, u, v, w
+    double* a[6];
+};
 cudaError_t launch_particles_heun(const double* const coefs[3], const SplineGrid& g, const DevClock* clock,
-                                  long long np, double* py, double* px, double* pz, double* Uu, double* Uv,
-                                  double* Uw, cudaStream_t s);
+                                  long long np, const ParticleArrays& src, const ParticleArrays& dst,
+                                  const long long* tag_src, long long* tag_dst, cudaStream_t s);
+// order the particles of src by blocks of 8^3 spline cells into dst (tags move with them);
+// keys: np values, counts: ((npts + 7) / 8)^3, temp: scan_temp_size(counts) values
+int scan_temp_size(long long n);
+cudaError_t launch_particle_sort(const SplineGrid& g, long long np, const ParticleArrays& src, const ParticleArrays& dst,
+                                 const long long* tag_src, long long* tag_dst, unsigned* keys, unsigned* counts,
+                                 unsigned* temp, int* launches, cudaStream_t s);
 
 struct StatsPartial {  // per-CTA partial sums of the PrintStats moments
     double v[16];

@@ -559,13 +559,14 @@ __global__ void particles_eval_kernel(Coefs3 cf, SplineGrid g, long long np, con
 // U2 from the new spline at pos + U dt (pos is (y, x, z), U is (u, v, w)),
 // pos += (U + U2) dt / 2, periodic wrap, then U at the new position for the
 // next step's predictor (the reference's getParticleProp at loop start).
+// particle p read from src and written to dst (the same arrays, or the sorted copy and the
+// particle arrays); arrays y, x, z, u, v, w
 __device__ __forceinline__ void heun_particle(const Coefs3& cf, const SplineGrid& g, double dt, long long p,
-                                              double* __restrict__ py, double* __restrict__ px, double* __restrict__ pz,
-                                              double* __restrict__ Uu, double* __restrict__ Uv, double* __restrict__ Uw)
+                                              const ParticleArrays& src, const ParticleArrays& dst)
 {
     const double twopi = 2.0 * 3.14159265358979311600;   // 2 * atan(1)*4 in double
-    double pos[3] = {py[p], px[p], pz[p]};
-    const double U[3] = {Uu[p], Uv[p], Uw[p]};
+    double pos[3] = {src.a[0][p], src.a[1][p], src.a[2][p]};
+    const double U[3] = {src.a[3][p], src.a[4][p], src.a[5][p]};
     double U2[3];
     eval3(cf.c, g, add(pos[0], mul(U[1], dt)), add(pos[1], mul(U[0], dt)), add(pos[2], mul(U[2], dt)), U2);
     pos[0] = add(pos[0], mul(mul(0.5, add(U[1], U2[1])), dt));
@@ -578,25 +579,106 @@ __device__ __forceinline__ void heun_particle(const Coefs3& cf, const SplineGrid
     }
     double Un[3];
     eval3(cf.c, g, pos[0], pos[1], pos[2], Un);
-    py[p] = pos[0];
-    px[p] = pos[1];
-    pz[p] = pos[2];
-    Uu[p] = Un[0];
-    Uv[p] = Un[1];
-    Uw[p] = Un[2];
+    dst.a[0][p] = pos[0];
+    dst.a[1][p] = pos[1];
+    dst.a[2][p] = pos[2];
+    dst.a[3][p] = Un[0];
+    dst.a[4][p] = Un[1];
+    dst.a[5][p] = Un[2];
 }
 
 // Heun step (src/ParticleTrack.cpp:48-73): U from the previous evaluation,
 // U2 from the new spline at pos + U dt (pos is (y, x, z), U is (u, v, w)),
 // pos += (U + U2) dt / 2, periodic wrap, then U at the new position for the
 // next step's predictor (the reference's getParticleProp at loop start).
+// With tag_src the particles come from the sorted copy and their tags move with them.
 __global__ void particles_heun_kernel(Coefs3 cf, SplineGrid g, const DevClock* __restrict__ clock, long long np,
-                                      double* __restrict__ py, double* __restrict__ px, double* __restrict__ pz,
-                                      double* __restrict__ Uu, double* __restrict__ Uv, double* __restrict__ Uw)
+                                      ParticleArrays src, ParticleArrays dst, const long long* __restrict__ tag_src,
+                                      long long* __restrict__ tag_dst)
 {
     const double dt = clock->dt;
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x)
-        heun_particle(cf, g, dt, p, py, px, pz, Uu, Uv, Uw);
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        heun_particle(cf, g, dt, p, src, dst);
+        if (tag_src) tag_dst[p] = tag_src[p];
+    }
+}
+
+// ------------------------------------------------------- particle ordering --
+// Particles are kept ordered by blocks of 8^3 spline cells (y-major, z fastest,
+// the coefficient layout), so the 4x4x4 windows that a warp gathers overlap
+// in L1/L2.  A counting sort: keys and counts, an exclusive scan of the
+// counts, a scatter into the second particle arrays.  Each particle's
+// arithmetic is independent of the order.
+__global__ void particle_keys_kernel(SplineGrid g, int nb, long long np, ParticleArrays P, unsigned* __restrict__ keys,
+                                     unsigned* __restrict__ counts)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        double t;
+        const int a = locate(g, P.a[0][p], t) >> 3, b = locate(g, P.a[1][p], t) >> 3, c = locate(g, P.a[2][p], t) >> 3;
+        const unsigned key = ((unsigned)a * nb + b) * nb + c;
+        keys[p] = key;
+        atomicAdd(&counts[key], 1u);
+    }
+}
+
+constexpr int kScanChunk = 1024;   // elements per CTA of the scan (256 threads x 4)
+
+// exclusive scan of data[0, n) in chunks of kScanChunk; chunk totals to sums (if given)
+__global__ void __launch_bounds__(256) scan_chunks_kernel(unsigned* __restrict__ data, long long n,
+                                                          unsigned* __restrict__ sums)
+{
+    __shared__ unsigned warp_tot[8];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const long long base = (long long)blockIdx.x * kScanChunk + 4LL * tid;
+    unsigned v[4], run = 0;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        v[e] = (base + e < n) ? data[base + e] : 0u;
+        run += v[e];
+    }
+    unsigned x = run;   // inclusive scan of the threads' totals within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned t = lane < 8 ? warp_tot[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < 8) warp_tot[lane] = t;
+    }
+    __syncthreads();
+    unsigned excl = x - run + (wid ? warp_tot[wid - 1] : 0u);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        if (base + e < n) data[base + e] = excl;
+        excl += v[e];
+    }
+    if (sums && tid == 0) sums[blockIdx.x] = warp_tot[7];
+}
+
+__global__ void scan_add_kernel(unsigned* __restrict__ data, long long n, const unsigned* __restrict__ sums)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        data[i] += sums[i / kScanChunk];
+}
+
+__global__ void particle_scatter_kernel(long long np, const unsigned* __restrict__ keys, unsigned* __restrict__ offsets,
+                                        ParticleArrays src, ParticleArrays dst, const long long* __restrict__ tag_src,
+                                        long long* __restrict__ tag_dst)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        const unsigned d = atomicAdd(&offsets[keys[p]], 1u);
+#pragma unroll
+        for (int c = 0; c < 6; c++) dst.a[c][d] = src.a[c][p];
+        tag_dst[d] = tag_src[p];
+    }
 }
 
 // ---------------------------------------------------------------- stats --
@@ -784,7 +866,8 @@ __global__ void ensemble_heun_kernel(const MemberDev* __restrict__ mem, const lo
         const int m = find_member(off, nm, x);
         const MemberDev& md = mem[m];
         const Coefs3 cf{{md.coef[0], md.coef[1], md.coef[2]}};
-        heun_particle(cf, md.grid, md.clock->dt, x - off[m], md.P[0], md.P[1], md.P[2], md.P[3], md.P[4], md.P[5]);
+        const ParticleArrays P{{md.P[0], md.P[1], md.P[2], md.P[3], md.P[4], md.P[5]}};
+        heun_particle(cf, md.grid, md.clock->dt, x - off[m], P, P);
     }
 }
 
@@ -890,12 +973,58 @@ cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid
 }
 
 cudaError_t launch_particles_heun(const double* const coefs[3], const SplineGrid& g, const DevClock* clock, long long np,
-                                  double* py, double* px, double* pz, double* Uu, double* Uv, double* Uw,
-                                  cudaStream_t s)
+                                  const ParticleArrays& src, const ParticleArrays& dst, const long long* tag_src,
+                                  long long* tag_dst, cudaStream_t s)
 {
     if (np <= 0) return cudaSuccess;
     Coefs3 cf{{coefs[0], coefs[1], coefs[2]}};
-    return grid_launch(particles_heun_kernel, np, 128, s, cf, g, clock, np, py, px, pz, Uu, Uv, Uw);
+    return grid_launch(particles_heun_kernel, np, 128, s, cf, g, clock, np, src, dst, tag_src, tag_dst);
+}
+
+int scan_temp_size(long long n)
+{
+    long long total = 0;
+    for (long long m = (n + kScanChunk - 1) / kScanChunk; m > 1; m = (m + kScanChunk - 1) / kScanChunk) total += m;
+    return (int)(total + 1);
+}
+
+// exclusive scan of data[0, n) in place; temp holds scan_temp_size(n) values
+static cudaError_t scan_exclusive(unsigned* data, long long n, unsigned* temp, int* launches, cudaStream_t s)
+{
+    const long long chunks = (n + kScanChunk - 1) / kScanChunk;
+    if (chunks <= 1) {
+        scan_chunks_kernel<<<1, 256, 0, s>>>(data, n, nullptr);
+        *launches += 1;
+        return cudaGetLastError();
+    }
+    scan_chunks_kernel<<<(unsigned)chunks, 256, 0, s>>>(data, n, temp);
+    *launches += 1;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = scan_exclusive(temp, chunks, temp + chunks, launches, s);
+    if (e != cudaSuccess) return e;
+    long long b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    scan_add_kernel<<<(unsigned)b, 256, 0, s>>>(data, n, temp);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_particle_sort(const SplineGrid& g, long long np, const ParticleArrays& src, const ParticleArrays& dst,
+                                 const long long* tag_src, long long* tag_dst, unsigned* keys, unsigned* counts,
+                                 unsigned* temp, int* launches, cudaStream_t s)
+{
+    if (np <= 0) return cudaSuccess;
+    const int nb = (g.npts + 7) / 8;
+    const long long nkeys = (long long)nb * nb * nb;
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(unsigned) * (size_t)nkeys, s);
+    if (e != cudaSuccess) return e;
+    e = grid_launch(particle_keys_kernel, np, 256, s, g, nb, np, src, keys, counts);
+    if (e != cudaSuccess) return e;
+    *launches += 1;   // the memset is a copy-engine operation, not a kernel
+    e = scan_exclusive(counts, nkeys, temp, launches, s);
+    if (e != cudaSuccess) return e;
+    return grid_launch(particle_scatter_kernel, np, 256, s, np, (const unsigned*)keys, counts, src, dst, tag_src, tag_dst);
 }
 
 cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const double* const coefs[3],
