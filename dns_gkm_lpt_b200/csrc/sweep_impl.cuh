@@ -117,10 +117,27 @@ __device__ __forceinline__ double block_max(double v, double* red)
 }
 
 template <class T, class Tile>
-constexpr size_t sweep_smem_bytes()
+__host__ __device__ constexpr size_t sweep_ring_bytes()
 {
-    return sizeof(T) * (size_t)(kRing * kSlabComps * Tile::WC + 10 * Tile::WC);
+    return (sizeof(T) * (size_t)(kRing * kSlabComps * Tile::WC + 10 * Tile::WC) + 15) / 16 * 16;
 }
+
+// ring + reconstructions, then a per-thread FP64 staging area [5][threads] for the
+// accumulator of the thread's cell, fetched asynchronously while the flux is computed
+template <class T, class Tile>
+__host__ __device__ constexpr size_t sweep_smem_bytes()
+{
+    return sweep_ring_bytes<T, Tile>() + sizeof(double) * 5 * (size_t)Tile::threads;
+}
+
+// cp.async: 8-byte global -> shared copies that land while the thread keeps computing
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 }  // namespace sweep_detail
 
@@ -176,6 +193,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     constexpr bool kMixed = sizeof(T) == 4;
     T* ring = reinterpret_cast<T*>(smem_raw);          // [kRing][kSlabComps][kWC]
     T* rec = ring + kRing * kSlabComps * kWC;          // [10][kWC]
+    double* stage = reinterpret_cast<double*>(smem_raw + sweep_ring_bytes<T, Tile>());   // [5][threads]
     const FieldConst& fc = a.fc;
     const int n = fc.n, nt = fc.nt;
     const long long nt3 = fc.nt3;
@@ -230,6 +248,30 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
         }
     };
 
+    // FP64: the slab of the next step travels global -> shared asynchronously during this step's
+    // flux (the ring slot it fills was last read by this step's reconstruction); its temperature
+    // is formed once the copies have landed
+    auto issue_slab = [&](int f) {
+        T* s = slot(f);
+        for (int c = tid; c < kWC; c += kSweepThreads) {
+            const int aa = c / kWB, bb = c - aa * kWB;
+            const int A = a0 + aa - 1, B = b0 + bb - 1;
+            if (A > n || B > n) continue;
+            const long long idx = (A + 3) * st.sA + (B + 3) * st.sB + (long long)(f + 3) * st.sn;
+#pragma unroll
+            for (int q = 0; q < 5; q++) cp_async8(&s[q * kWC + c], &W[q * nt3 + idx]);
+        }
+        cp_async_commit();
+    };
+    auto finish_slab = [&](int f) {
+        T* s = slot(f);
+        for (int c = tid; c < kWC; c += kSweepThreads) {
+            const int aa = c / kWB, bb = c - aa * kWB;
+            if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
+            s[5 * kWC + c] = temperature<T>(s[c], s[kWC + c], s[2 * kWC + c], s[3 * kWC + c], s[4 * kWC + c], ph);
+        }
+    };
+
     for (int f = f_begin - 3; f < f_begin + 2; f++) load_slab(f);
 
     const bool active = (a0 + ty < n) && (b0 + tx < n);
@@ -240,7 +282,12 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     bool bad = false;
 
     for (int f = f_begin - 1; f < f_end; f++) {
-        load_slab(f + 3);
+        if (kMixed || f == f_begin - 1) {
+            load_slab(f + 3);
+        } else {
+            cp_async_wait_all();
+            finish_slab(f + 3);
+        }
         __syncthreads();
         // reconstruct every face of the window once (the reference repeats this 5x per face)
         {
@@ -274,6 +321,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             }
         }
         __syncthreads();
+        if (!kMixed && f + 1 < f_end) issue_slab(f + 4);
         if (active) {
             SmemFace<DIR, T, kWC> pv;
             pv.wf = slot(f);
@@ -302,8 +350,18 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 double Tk = p / (kR * d);
                 tau0 = viscosity(fc, Tk) / p;
             }
+            const long long ci = cell0 + (long long)(f + 3) * st.sn;
+            // the accumulator of this cell (y, z sweeps) travels to shared memory while the flux
+            // is computed
+            const bool fetch_a = DIR != 0 && f >= f_begin;
+            if (fetch_a) {
+#pragma unroll
+                for (int q = 0; q < 5; q++) cp_async8(&stage[q * kSweepThreads + tid], &a.A[q * nt3 + ci]);
+                cp_async_commit();
+            }
             T Fr[5];
             gks_flux<T>(pv, tau0, dtw, dxw, ph, Fr);
+            if (fetch_a) cp_async_wait_all();
             double F[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) {
@@ -311,23 +369,24 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 else F[perm<DIR>(q)] = Fr[q];
             }
             if (f >= f_begin) {
-                const long long ci = cell0 + (long long)(f + 3) * st.sn;
                 if (DIR == 0) {
 #pragma unroll
                     for (int q = 0; q < 5; q++) a.A[q * nt3 + ci] = __dsub_rn(F[q], Fprev[q]);
                 } else if (DIR == 1) {
 #pragma unroll
                     for (int q = 0; q < 5; q++) {
-                        double acc = a.A[q * nt3 + ci];
+                        double acc = stage[q * kSweepThreads + tid];
                         a.A[q * nt3 + ci] = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
                     }
                 } else {
                     double wn[5];
 #pragma unroll
                     for (int q = 0; q < 5; q++) {
-                        double acc = a.A[q * nt3 + ci];
+                        double acc = stage[q * kSweepThreads + tid];
                         double s = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
-                        wn[q] = __dsub_rn(W[q * nt3 + ci], __dmul_rn(fc.inv_dx, s));
+                        // the cell's FP64 state (the FP64 ring holds it; the mixed ring has FP32 copies)
+                        const double wq = kMixed ? W[q * nt3 + ci] : (double)wl[q * kWC + cc];
+                        wn[q] = __dsub_rn(wq, __dmul_rn(fc.inv_dx, s));
                         a.A[q * nt3 + ci] = wn[q];
                     }
                     double ws = wave_speed(wn, fc.gam, fc.gm1);
