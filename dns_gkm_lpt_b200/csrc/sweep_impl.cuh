@@ -89,6 +89,18 @@ __device__ __forceinline__ double viscosity(const FieldConst& fc, double T)
 }
 
 // max(|u| + c) term of one cell with the reference's rounding (src/update.cpp:844-853,1041-1048)
+// |u| + c of a conserved state in FP64.  The mixed form (whose fields carry FP32 flux errors
+// anyway) takes one reciprocal of rho instead of five divisions; the FP64 drop-in keeps the
+// reference's divisions (src/update.cpp:1039-1046 via c2p), so its dt is the reference's bit for bit.
+__device__ __forceinline__ double wave_speed_recip(const double w[5], double gam, double gm1)
+{
+    const double d = w[0], id = 1.0 / d;
+    const double u = w[1] * id, v = w[2] * id, x = w[3] * id;
+    const double vs = u * u + v * v + x * x;
+    const double p = (d * gm1) * (w[4] * id - 0.5 * vs);
+    return sqrt(vs) + sqrt(gam * p * id);
+}
+
 __device__ __forceinline__ double wave_speed(const double w[5], double gam, double gm1)
 {
     double d = w[0];
@@ -249,17 +261,18 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     };
 
     // FP64: the slab of the next step travels global -> shared asynchronously during this step's
-    // flux (the ring slot it fills was last read by this step's reconstruction); its temperature
-    // is formed once the copies have landed
+    // flux, straight into its ring slot (last read by this step's reconstruction); each thread
+    // forms the temperature of the cells it copied once its copies have landed.  (The mixed form
+    // converts while loading; an asynchronous landing area measured slower there.)
     auto issue_slab = [&](int f) {
-        T* s = slot(f);
+        double* dst = reinterpret_cast<double*>(slot(f));
         for (int c = tid; c < kWC; c += kSweepThreads) {
             const int aa = c / kWB, bb = c - aa * kWB;
             const int A = a0 + aa - 1, B = b0 + bb - 1;
             if (A > n || B > n) continue;
             const long long idx = (A + 3) * st.sA + (B + 3) * st.sB + (long long)(f + 3) * st.sn;
 #pragma unroll
-            for (int q = 0; q < 5; q++) cp_async8(&s[q * kWC + c], &W[q * nt3 + idx]);
+            for (int q = 0; q < 5; q++) cp_async8(&dst[q * kWC + c], &W[q * nt3 + idx]);
         }
         cp_async_commit();
     };
@@ -352,8 +365,10 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             }
             const long long ci = cell0 + (long long)(f + 3) * st.sn;
             // the accumulator of this cell (y, z sweeps) travels to shared memory while the flux
-            // is computed
-            const bool fetch_a = DIR != 0 && f >= f_begin;
+            // is computed (the mixed z sweep, which also re-reads the state, loads it directly:
+            // measured faster there)
+            constexpr bool kFetchA = DIR == 1 || (DIR == 2 && !kMixed);
+            const bool fetch_a = kFetchA && f >= f_begin;
             if (fetch_a) {
 #pragma unroll
                 for (int q = 0; q < 5; q++) cp_async8(&stage[q * kSweepThreads + tid], &a.A[q * nt3 + ci]);
@@ -382,14 +397,14 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                     double wn[5];
 #pragma unroll
                     for (int q = 0; q < 5; q++) {
-                        double acc = stage[q * kSweepThreads + tid];
+                        double acc = kFetchA ? stage[q * kSweepThreads + tid] : a.A[q * nt3 + ci];
                         double s = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
                         // the cell's FP64 state (the FP64 ring holds it; the mixed ring has FP32 copies)
                         const double wq = kMixed ? W[q * nt3 + ci] : (double)wl[q * kWC + cc];
                         wn[q] = __dsub_rn(wq, __dmul_rn(fc.inv_dx, s));
                         a.A[q * nt3 + ci] = wn[q];
                     }
-                    double ws = wave_speed(wn, fc.gam, fc.gm1);
+                    double ws = kMixed ? wave_speed_recip(wn, fc.gam, fc.gm1) : wave_speed(wn, fc.gam, fc.gm1);
                     if (!isfinite(ws) || !(wn[0] > 0.0)) bad = true;
                     else wmax = ws > wmax ? ws : wmax;
                 }
