@@ -538,7 +538,7 @@ gkm_status gkm_destroy(gkm_handle* h)
     cudaFree(h->lap_nodes);
     cudaFree(h->props);
     for (cudaEvent_t e : h->pipe_ev) cudaEventDestroy(e);
-    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1]})
+    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1], h->pipe_comp[2], h->pipe_comp[3]})
         if (s) cudaStreamDestroy(s);
     cudaFree(h->partials);
     cudaFree(h->stats_out);
@@ -783,11 +783,13 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     const FieldConst& fc = h->fc;
     const int n = fc.n;
     const size_t plane = (size_t)fc.nt * fc.nt, nt3 = (size_t)fc.nt3;
-    int C = ((n / 8 + 15) / 16) * 16;   // a multiple of every window height, about n/8
+    int C = h->pipe_chunk ? h->pipe_chunk : ((n / 8 + 15) / 16) * 16;   // a multiple of every window height
     if (C < 16) C = 16;
     const int K = (n + C - 1) / C;
+    const int S = h->pipe_streams;
     if (!h->pipe_in) {
-        for (cudaStream_t* s : {&h->pipe_in, &h->pipe_out, &h->pipe_comp[0], &h->pipe_comp[1]})
+        for (cudaStream_t* s : {&h->pipe_in, &h->pipe_out, &h->pipe_comp[0], &h->pipe_comp[1], &h->pipe_comp[2],
+                                &h->pipe_comp[3]})
             CK(h, cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
     }
     const size_t nev = 2 * (size_t)K + 2;
@@ -809,7 +811,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     CK(h, cudaMemsetAsync(&ck->wave[h->parity ^ 1], 0, sizeof(unsigned long long), h->stream));
     CK(h, cudaMemsetAsync(&ck->status, 0, sizeof(int), h->stream));
     CK(h, cudaEventRecord(ev_start, h->stream));
-    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1]})
+    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1], h->pipe_comp[2], h->pipe_comp[3]})
         CK(h, cudaStreamWaitEvent(s, ev_start, 0));
 
     auto copy_in = [&](int J0, int J1) -> cudaError_t {
@@ -847,7 +849,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
         CK(h, cudaEventRecord(ev_in[c], h->pipe_in));
     }
 
-    // compute: chunk c on compute stream c % 2, after the copy-in of chunk c+1
+    // compute: chunk c on compute stream c % S, after the copy-in of chunk c+1
     gkm::SweepArgs a{};
     a.W = Wd;
     a.A = A;
@@ -858,7 +860,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     a.dt_fixed = dt;
     a.skip_clock_init = 1;
     for (int c = 0; c < K; c++) {
-        cudaStream_t s = h->pipe_comp[c % 2];
+        cudaStream_t s = h->pipe_comp[c % S];
         CK(h, cudaStreamWaitEvent(s, ev_in[std::min(c + 1, K - 1)], 0));
         const int j0 = c * C, j1 = std::min((c + 1) * C, n);
         for (int d = 0; d < 3; d++) {
@@ -892,6 +894,16 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
 }
 
 }  // namespace
+
+gkm_status gkm_set_pipeline(gkm_handle* h, int32_t chunk_planes, int32_t compute_streams)
+{
+    if (!h) return GKM_ERR_ARG;
+    if (chunk_planes < 0 || chunk_planes % 16 || compute_streams < 1 || compute_streams > 4)
+        return fail(h, GKM_ERR_ARG, "chunk_planes: 0 or a multiple of 16; compute_streams: 1..4");
+    h->pipe_chunk = chunk_planes;
+    h->pipe_streams = compute_streams;
+    return GKM_OK;
+}
 
 gkm_status gkm_evolve(gkm_handle* h, double* const W[5], double dt)
 {

@@ -60,8 +60,10 @@ struct gkm_handle {
     int64_t launches = 0;    // kernels launched (graph replays add the kernels they hold)
     // plug-point pipeline (gkm_evolve with pinned or device buffers): copy-in, copy-out and
     // two compute streams, and per-chunk events, created on first use
-    cudaStream_t pipe_in = nullptr, pipe_out = nullptr, pipe_comp[2] = {nullptr, nullptr};
+    cudaStream_t pipe_in = nullptr, pipe_out = nullptr, pipe_comp[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> pipe_ev;
+    int pipe_chunk = 0;      // y-planes per chunk (multiple of 16); 0: about n/8
+    int pipe_streams = 2;    // compute streams
     std::string err;
     gkm_ensemble* owner = nullptr;   // set while the handle is a member of an ensemble
 };

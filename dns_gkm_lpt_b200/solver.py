@@ -141,6 +141,10 @@ class Solver:
         """The reference GPU plug point evolve(W, dev, dt): W updated in place."""
         self._check(self.L.gkm_evolve(self.h, _w5(W), dt))
 
+    def set_pipeline(self, chunk_planes: int = 0, compute_streams: int = 2) -> None:
+        """Shape of the evolve() pipeline used with pinned or device buffers."""
+        self._check(self.L.gkm_set_pipeline(self.h, chunk_planes, compute_streams))
+
     def step(self, nsteps: int = 1) -> None:
         self._check(self.L.gkm_step(self.h, nsteps))
 

@@ -139,6 +139,9 @@ gkm_status gkm_evolve_eulerian(gkm_handle* h, int32_t nsteps);
  * copies in and out overlap the sweeps; pageable W takes one copy in, the
  * step, one copy out.  Both give the same result. */
 gkm_status gkm_evolve(gkm_handle* h, double* const W[5], double dt);
+/* Shape of that pipeline (no reference counterpart): y-planes per chunk (a
+ * multiple of 16; 0 picks about n/8) and compute streams (1..4, default 2). */
+gkm_status gkm_set_pipeline(gkm_handle* h, int32_t chunk_planes, int32_t compute_streams);
 
 /* nsteps of the body of Evolve's loop (src/update.cpp:124-170): Eulerian
  * step, velocity splines of the new state (generateSplines, :1235-1247),
