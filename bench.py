@@ -61,6 +61,20 @@ def ensemble_specs():
     return specs
 
 
+def max_over_ranks(values, device=None):
+    """Element-wise maximum of per-rank timings over all ranks of the default process group
+    (identity without one).  Every rank must call it, in the same order, with the same length."""
+    import torch
+    import torch.distributed as tdist
+    if not (tdist.is_available() and tdist.is_initialized()) or tdist.get_world_size() == 1:
+        return [float(v) for v in values]
+    if device is None:
+        device = "cuda" if tdist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def cells_of(n: int) -> int:
     return n ** 3
 
@@ -329,10 +343,7 @@ def ours(args, rank: int, world: int, local_rank: int):
     total_ms = e0.elapsed_time(e1)
     eul_ms = ph["sweep_x"] + ph["sweep_y"] + ph["sweep_z"] + ph["halo"]
     part_ms = ph["splines"] + ph["particles"]
-    if dist:
-        t = torch.tensor([eul_ms, part_ms, total_ms], dtype=torch.float64, device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        eul_ms, part_ms, total_ms = t.tolist()
+    eul_ms, part_ms, total_ms = max_over_ranks([eul_ms, part_ms, total_ms])
     nt = s.nt
     state_bytes = 5 * nt ** 3 * 8
     do_forms = not args.no_forms and prec == 0
@@ -357,11 +368,8 @@ def ours(args, rank: int, world: int, local_rank: int):
             s.evolve(Wn, dt)
         x1.record(stream)
         torch.cuda.synchronize()
-        e2e_ms = x0.elapsed_time(x1)
+        e2e_ms = max_over_ranks([x0.elapsed_time(x1)])[0]
         if dist:
-            t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-            e2e_ms = t.item()
             tdist.barrier()
         del Wh, Wn
         e2e = {"value": world * n ** 3 * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
@@ -386,9 +394,10 @@ def ours(args, rank: int, world: int, local_rank: int):
         sl = slice(3, -3)
         err = [float(np.linalg.norm(Wm[q, sl, sl, sl] - W64[q, sl, sl, sl]) / np.linalg.norm(W64[q, sl, sl, sl]))
                for q in range(5)]
-        m_eul = mph["sweep_x"] + mph["sweep_y"] + mph["sweep_z"] + mph["halo"]
+        m_eul, m_part = max_over_ranks([mph["sweep_x"] + mph["sweep_y"] + mph["sweep_z"] + mph["halo"],
+                                        mph["splines"] + mph["particles"]])
         forms["mixed"] = {"value": world * n ** 3 * args.steps / (m_eul * 1e-3) / 1e9, "unit": "Gcell-updates/s",
-                          "particle_steps_per_s": world * npart * args.steps / ((mph["splines"] + mph["particles"]) * 1e-3),
+                          "particle_steps_per_s": world * npart * args.steps / (m_part * 1e-3),
                           "ms_per_step": mph["total"] / args.steps,
                           "phases_ms_per_step": {k: v / args.steps for k, v in mph.items()},
                           "rel_l2_vs_fp64": dict(zip(("rho", "rho_u", "rho_v", "rho_w", "rho_E"), err)),
