@@ -9,6 +9,8 @@
 #include "gkm.h"
 #include "gkm_handle.h"
 
+#include <cuda.h>   // CUtensorMap and its enums (the encoder comes from the driver at run time)
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -93,10 +95,62 @@ void destroy_graphs(gkm_handle* h)
         }
 }
 
+// tensor map of the state buffer W for sweep direction dir and window variant (FP64 x, y)
+const void* sweep_tmap(const gkm_handle* h, const double* W, int dir, int variant)
+{
+    if (!h->d_tmaps || dir > 1 || h->cfg.precision == GKM_PREC_MIXED) return nullptr;
+    const int b = (W == h->buf[0]) ? 0 : (W == h->buf[1] ? 1 : -1);
+    if (b < 0) return nullptr;
+    return h->d_tmaps + sizeof(CUtensorMap) * (size_t)((b * gkm::kSweepVariants64 + variant) * 2 + dir);
+}
+
+// Encode the tensor maps: W as a 4-D tensor (k, i, j, q) of doubles, dims (nt, nt, nt, 5); box
+// (WB, 1, WA, 5) for the x sweep (window j x k at one i) and (WB, WA, 1, 5) for the y sweep
+// (window i x k at one j).  The row strides must be multiples of 16 bytes, so nt must be even;
+// otherwise (or without the driver entry point) the sweeps copy slabs with cp.async.
+cudaError_t setup_tensor_maps(gkm_handle* h)
+{
+    if (h->cfg.precision == GKM_PREC_MIXED || h->fc.nt % 2) return cudaSuccess;
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+        cudaGetLastError();
+        return cudaSuccess;
+    }
+    const Encode encode = reinterpret_cast<Encode>(fn);
+    const cuuint64_t nt = (cuuint64_t)h->fc.nt;
+    const cuuint64_t dims[4] = {nt, nt, nt, 5};
+    const cuuint64_t strides[3] = {nt * 8, nt * nt * 8, nt * nt * nt * 8};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const int nmaps = 2 * gkm::kSweepVariants64 * 2;
+    std::vector<CUtensorMap> maps((size_t)nmaps);
+    for (int b = 0; b < 2; b++)
+        for (int v = 0; v < gkm::kSweepVariants64; v++)
+            for (int d = 0; d < 2; d++) {
+                const gkm::SweepShape sh = gkm::sweep_shape(false, v);
+                const cuuint32_t WB = (cuuint32_t)sh.TB + 2, WA = (cuuint32_t)sh.TA + 2;
+                const cuuint32_t box[4] = {WB, d == 0 ? 1u : WA, d == 0 ? WA : 1u, 5};
+                CUresult r = encode(&maps[(size_t)((b * gkm::kSweepVariants64 + v) * 2 + d)],
+                                    CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, h->buf[b], dims, strides, box, estr,
+                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r != CUDA_SUCCESS) return cudaSuccess;   // keep the cp.async path
+            }
+    cudaError_t e = cudaMalloc(&h->d_tmaps, sizeof(CUtensorMap) * (size_t)nmaps);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(h->d_tmaps, maps.data(), sizeof(CUtensorMap) * (size_t)nmaps, cudaMemcpyHostToDevice);
+    return e;
+}
+
 cudaError_t launch_sweep_any(gkm_handle* h, int dir, gkm::SweepArgs a)
 {
     const SweepChoice& c = h->sweep[dir];
     a.seg_len = c.seg_len;
+    a.tmap = sweep_tmap(h, a.W, dir, c.variant);
     if (h->cfg.precision == GKM_PREC_MIXED) return gkm::launch_sweep_mixed(dir, c.variant, a, c.nseg, h->stream);
     return gkm::launch_sweep(dir, c.variant, a, c.nseg, h->stream);
 }
@@ -287,6 +341,7 @@ gkm_status read_clock(gkm_handle* h, DevClock* c)
 {
     CK(h, cudaMemcpyAsync(c, h->clock, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
+    if (c->status & 2) return fail(h, GKM_ERR_CUDA, "a bulk tensor copy of a sweep did not complete in time");
     if (c->status & 1) return fail(h, GKM_ERR_NONFINITE, "state holds a non-finite value or non-positive density");
     return GKM_OK;
 }
@@ -507,6 +562,8 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     if (e != cudaSuccess) return bail(e, "sweep_prepare");
     e = setup_batched_splines(h);
     if (e != cudaSuccess) return bail(e, "batched spline build");
+    e = setup_tensor_maps(h);
+    if (e != cudaSuccess) return bail(e, "tensor maps");
     *out = h;
     return GKM_OK;
 }
@@ -525,6 +582,7 @@ gkm_status gkm_destroy(gkm_handle* h)
     for (int k = 0; k < 2; k++) cudaFree(h->scratch_extra[k]);
     cudaFree(h->d_self);
     cudaFree(h->d_self_off);
+    cudaFree(h->d_tmaps);
     for (int c = 0; c < 6; c++) {
         cudaFree(h->P[c]);
         cudaFree(h->P_sorted[c]);
@@ -867,6 +925,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
             gkm::SweepArgs ad = a;
             ad.seg_len = (d == 1) ? C : h->sweep[d].seg_len;
             const int v = h->sweep[d].variant;
+            ad.tmap = sweep_tmap(h, ad.W, d, v);
             CK(h, mixed ? gkm::launch_sweep_mixed_rows(d, v, ad, j0, j1, s) : gkm::launch_sweep_rows(d, v, ad, j0, j1, s));
         }
         CK(h, gkm::launch_halo_planes(A, fc, 3 + j0, 3 + j1, s));

@@ -63,6 +63,9 @@ struct gkm_handle {
     cudaStream_t pipe_in = nullptr, pipe_out = nullptr, pipe_comp[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> pipe_ev;
     int pipe_chunk = 0;      // y-planes per chunk (multiple of 16); 0: about n/8
+    // tensor maps of the two state buffers for the FP64 x / y sweeps' slab copies, in device
+    // memory, index (buffer * kSweepVariants64 + variant) * 2 + direction; null when unavailable
+    unsigned char* d_tmaps = nullptr;
     int pipe_streams = 2;    // compute streams
     std::string err;
     gkm_ensemble* owner = nullptr;   // set while the handle is a member of an ensemble

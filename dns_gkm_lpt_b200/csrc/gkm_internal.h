@@ -81,6 +81,7 @@ struct SweepArgs {
     int tile_a0;                    // first window row (x, z sweeps) of a launch over part of the j range
     int seg0;                       // first segment (y sweep) of such a launch
     int skip_clock_init;            // 1: the clock's dt and next wave slot were set before the launch
+    const void* tmap;               // FP64 x / y sweeps: tensor map of W for the slab copies (else null)
 };
 
 // kernel launchers (sweep.cu); sweep_prepare sets the sweep kernels' shared-memory limit once

@@ -128,10 +128,19 @@ __device__ __forceinline__ double block_max(double v, double* red)
     return v;
 }
 
+// elements of one ring slot: kSlabComps x WC values, padded to a multiple of 128 bytes
+template <class T, class Tile>
+__host__ __device__ constexpr int slot_elems()
+{
+    return (int)((kSlabComps * Tile::WC * sizeof(T) + 127) / 128 * 128 / sizeof(T));
+}
+
 template <class T, class Tile>
 __host__ __device__ constexpr size_t sweep_ring_bytes()
 {
-    return (sizeof(T) * (size_t)(kRing * kSlabComps * Tile::WC + 10 * Tile::WC) + 15) / 16 * 16;
+    // 128 bytes of slack to align the ring (a bulk tensor copy lands on a 128-byte boundary),
+    // the ring of padded slots, the reconstructions
+    return (128 + sizeof(T) * (size_t)(kRing * slot_elems<T, Tile>() + 10 * Tile::WC) + 15) / 16 * 16;
 }
 
 // ring + reconstructions, then a per-thread FP64 staging area [5][threads] for the
@@ -139,7 +148,7 @@ __host__ __device__ constexpr size_t sweep_ring_bytes()
 template <class T, class Tile>
 __host__ __device__ constexpr size_t sweep_smem_bytes()
 {
-    return sweep_ring_bytes<T, Tile>() + sizeof(double) * 5 * (size_t)Tile::threads;
+    return sweep_ring_bytes<T, Tile>() + sizeof(double) * 5 * (size_t)Tile::threads + 16;   // + mbarrier
 }
 
 // cp.async: 8-byte global -> shared copies that land while the thread keeps computing
@@ -149,6 +158,41 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+// Bulk tensor copies (TMA) completing on an mbarrier.  The waits are bounded: a copy that has not
+// landed after ~2^24 polls raises bit 1 of the clock's status word and the kernel carries on,
+// so a failure is reported to the host and never hangs the GPU.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void tma_slab_load(unsigned dst, const void* tmap, int c0, int c1, int c2, unsigned bytes,
+                                              unsigned bar)
+{
+    // shared-memory writes of the generic proxy (the slot's previous contents) before the copy's
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(dst),
+        "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(0), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
+{
+    for (int it = 0; it < (1 << 24); it++) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 }  // namespace sweep_detail
@@ -203,9 +247,13 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     constexpr int kTB = Tile::TB, kTA = Tile::TA, kWB = Tile::WB, kWC = Tile::WC;
     constexpr int kSweepThreads = Tile::threads;
     constexpr bool kMixed = sizeof(T) == 4;
-    T* ring = reinterpret_cast<T*>(smem_raw);          // [kRing][kSlabComps][kWC]
-    T* rec = ring + kRing * kSlabComps * kWC;          // [10][kWC]
+    constexpr int kSlot = slot_elems<T, Tile>();
+    // ring [kRing][kSlot] (slot: kSlabComps x kWC values), reconstructions [10][kWC], then the
+    // accumulator staging [5][threads] and one mbarrier
+    T* ring = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    T* rec = ring + kRing * kSlot;
     double* stage = reinterpret_cast<double*>(smem_raw + sweep_ring_bytes<T, Tile>());   // [5][threads]
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(stage + 5 * kSweepThreads);
     const FieldConst& fc = a.fc;
     const int n = fc.n, nt = fc.nt;
     const long long nt3 = fc.nt3;
@@ -231,7 +279,18 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     }
     if (f_begin >= n) return;
 
-    auto slot = [&](int f) { return ring + ((f + 12) % kRing) * (kSlabComps * kWC); };
+    // FP64 x and y sweeps with a tensor map: one thread moves each new slab (5 components of the
+    // window, a box of the (k, i, j, q) tensor whose smem image is the slot's [q][a][b] layout)
+    // with one bulk tensor copy completing on the mbarrier
+    const bool use_tma = !kMixed && DIR != 2 && a.tmap != nullptr;
+    const unsigned bar_u32 = smem_u32(bar);
+    unsigned tma_phase = 0;
+    if (use_tma) {
+        if (tid == 0) mbar_init(bar_u32);
+        __syncthreads();
+    }
+
+    auto slot = [&](int f) { return ring + ((f + 12) % kRing) * kSlot; };
     auto load_slab = [&](int f) {
         T* s = slot(f);
         for (int c = tid; c < kWC; c += kSweepThreads) {
@@ -298,7 +357,12 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
         if (kMixed || f == f_begin - 1) {
             load_slab(f + 3);
         } else {
-            cp_async_wait_all();
+            if (use_tma) {
+                if (!mbar_wait_bounded(bar_u32, tma_phase)) atomicOr(&a.clock->status, 2);
+                tma_phase ^= 1u;
+            } else {
+                cp_async_wait_all();
+            }
             finish_slab(f + 3);
         }
         __syncthreads();
@@ -334,7 +398,18 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             }
         }
         __syncthreads();
-        if (!kMixed && f + 1 < f_end) issue_slab(f + 4);
+        if (!kMixed && f + 1 < f_end) {
+            if (use_tma) {
+                if (tid == 0) {
+                    // box origin: window row a0-1, column b0-1 (ghost-layout +3), normal plane f+4
+                    const int cb = b0 + 2, ca = a0 + 2, cn = f + 4 + 3;
+                    tma_slab_load(smem_u32(slot(f + 4)), a.tmap, cb, DIR == 0 ? cn : ca, DIR == 0 ? ca : cn,
+                                  (unsigned)(5 * kWC * sizeof(double)), bar_u32);
+                }
+            } else {
+                issue_slab(f + 4);
+            }
+        }
         if (active) {
             SmemFace<DIR, T, kWC> pv;
             pv.wf = slot(f);
@@ -446,6 +521,7 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
         const int bz = (int)(local % nseg);
         const long long t = local / nseg;
         SweepArgs a;
+        a.tmap = nullptr;
         a.tile_a0 = 0;
         a.seg0 = 0;
         a.skip_clock_init = 0;
