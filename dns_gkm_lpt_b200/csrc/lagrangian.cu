@@ -24,22 +24,48 @@ __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, 
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 
 // One line: f (N points, stride fs) -> c (N+pad values, stride cs).
+// The recurrences are sequential, but their inputs are not: the loops fetch kLineBatch inputs
+// ahead (data in the forward sweeps, the forward results in the backward sweeps) so that many
+// loads are in flight per thread; the arithmetic and its order are unchanged.
+constexpr int kLineBatch = 8;
+
 template <class Src>
 __device__ void line_solve(const Src& f, int N, int periodic, const SplineTables& tb, double* c, long long cs)
 {
+    constexpr int U = kLineBatch;
     if (!periodic) {
         const double c0 = f(0), cl = f(N - 1);
         double rp = 0.0;
-        for (int i = 1; i <= N - 2; i++) {
-            double r = mul(6.0, f(i));
+        auto fwd = [&](int i, double fi) {
+            double r = mul(6.0, fi);
             if (i == 1) r = sub(r, c0);
             if (i == N - 2) r = sub(r, cl);
             rp = (i == 1) ? r : sub(r, mul(tb.mt[i], rp));
             c[(long long)(i + 1) * cs] = rp;
+        };
+        int i = 1;
+        for (; i + U - 1 <= N - 2; i += U) {
+            double fv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) fv[u] = f(i + u);
+#pragma unroll
+            for (int u = 0; u < U; u++) fwd(i + u, fv[u]);
         }
+        for (; i <= N - 2; i++) fwd(i, f(i));
         double x = __ddiv_rn(c[(long long)(N - 1) * cs], tb.dp[N - 2]);
         c[(long long)(N - 1) * cs] = x;
-        for (int i = N - 3; i >= 1; i--) {
+        i = N - 3;
+        for (; i - U + 1 >= 1; i -= U) {
+            double cv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) cv[u] = c[(long long)(i - u + 1) * cs];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                x = __ddiv_rn(sub(cv[u], x), tb.dp[i - u]);
+                c[(long long)(i - u + 1) * cs] = x;
+            }
+        }
+        for (; i >= 1; i--) {
             x = __ddiv_rn(sub(c[(long long)(i + 1) * cs], x), tb.dp[i]);
             c[(long long)(i + 1) * cs] = x;
         }
@@ -54,13 +80,35 @@ __device__ void line_solve(const Src& f, int N, int periodic, const SplineTables
         // y = B^-1 (6 f) stored in slots 1..N
         double rp = mul(6.0, f(0));
         c[cs] = rp;
-        for (int i = 1; i < N; i++) {
+        int i = 1;
+        for (; i + U - 1 <= N - 1; i += U) {
+            double fv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) fv[u] = f(i + u);
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                rp = sub(mul(6.0, fv[u]), mul(tb.mt[i + u], rp));
+                c[(long long)(i + u + 1) * cs] = rp;
+            }
+        }
+        for (; i < N; i++) {
             rp = sub(mul(6.0, f(i)), mul(tb.mt[i], rp));
             c[(long long)(i + 1) * cs] = rp;
         }
         double x = __ddiv_rn(c[(long long)N * cs], tb.dp[N - 1]);
         c[(long long)N * cs] = x;
-        for (int i = N - 2; i >= 0; i--) {
+        i = N - 2;
+        for (; i - U + 1 >= 0; i -= U) {
+            double cv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) cv[u] = c[(long long)(i - u + 1) * cs];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                x = __ddiv_rn(sub(cv[u], x), tb.dp[i - u]);
+                c[(long long)(i - u + 1) * cs] = x;
+            }
+        }
+        for (; i >= 0; i--) {
             x = __ddiv_rn(sub(c[(long long)(i + 1) * cs], x), tb.dp[i]);
             c[(long long)(i + 1) * cs] = x;
         }
