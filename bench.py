@@ -349,7 +349,10 @@ def ours(args, rank: int, world: int, local_rank: int):
     do_forms = not args.no_forms and prec == 0
     if do_forms:   # FP64 state after warmup + steps, the reference point of the mixed form
         W64 = s.download_state()
-        tke64 = s.print_stats()["TKE"]
+        st64 = s.print_stats()
+        tke64 = st64["TKE"]
+        pos64, _ = s.particles_download()
+        pst64 = s.particle_stats()
 
     # end to end through the plug point evolve(W, dt): pinned host W in, one step, W out
     e2e = None
@@ -389,7 +392,10 @@ def ours(args, rank: int, world: int, local_rank: int):
         m.step_timed(args.warmup, True)
         mph = m.step_timed(args.steps, True)
         Wm = m.download_state()
-        tkem = m.print_stats()["TKE"]
+        stm = m.print_stats()
+        tkem = stm["TKE"]
+        posm, _ = m.particles_download()
+        pstm = m.particle_stats()
         m.close()
         sl = slice(3, -3)
         err = [float(np.linalg.norm(Wm[q, sl, sl, sl] - W64[q, sl, sl, sl]) / np.linalg.norm(W64[q, sl, sl, sl]))
@@ -402,6 +408,15 @@ def ours(args, rank: int, world: int, local_rank: int):
                           "phases_ms_per_step": {k: v / args.steps for k, v in mph.items()},
                           "rel_l2_vs_fp64": dict(zip(("rho", "rho_u", "rho_v", "rho_w", "rho_E"), err)),
                           "tke_rel_err_vs_fp64": abs(tkem - tke64) / tke64,
+                          # every PrintStats statistic and the particles, against the FP64 run
+                          "stats_rel_err_vs_fp64": {k: abs(stm[k] - st64[k]) / max(abs(st64[k]), 1e-300)
+                                                    for k in st64 if k != "t_over_t0"},
+                          "t_over_t0_rel_err_vs_fp64": abs(stm["t_over_t0"] - st64["t_over_t0"]) / st64["t_over_t0"],
+                          "particle_stats_rel_err_vs_fp64": {k: abs(pstm[k] - pst64[k]) / max(abs(pst64[k]), 1e-300)
+                                                             for k in ("TKE", "SijSij", "SKEWu", "SKEWw")},
+                          "particle_pos_max_abs_err_vs_fp64": float(np.abs(posm - pos64).max()),
+                          "particle_cells_equal_fraction": float(np.mean(np.all(
+                              np.floor(posm / P.dx) == np.floor(pos64 / P.dx), axis=1))),
                           "steps_compared": args.warmup + args.steps, "sweep_shapes": m_cfg}
         del W64, Wm
         if not args.no_batched:
