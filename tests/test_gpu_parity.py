@@ -129,6 +129,34 @@ def test_64cube_step_matches_oracle(oracle):
         assert rel_l2(s.download_state(), Wo).max() <= FIELD_TOL
 
 
+def _analytic_case(n, seed):
+    """A smooth random-phase velocity field for any n (odd included; the spectral generator
+    needs even n): the odd grids take the cp.async slab copies instead of tensor-map copies."""
+    rng = np.random.default_rng(seed)
+    P = ic.Params(n=n, gam=1.4, den0=1.0, Mt=0.3, Re=30.0, mu0=0.9, p0=86100.0, t0=0.01)
+    x = (np.arange(n) + 0.5) * (2 * np.pi / n)
+    Y, X, Z = np.meshgrid(x, x, x, indexing="ij")
+    u, v, w = [sum(rng.uniform(20, 60) * np.sin(kx * X + ky * Y + kz * Z + rng.uniform(0, 2 * np.pi))
+                   for kx, ky, kz in ((1, 0, 1), (0, 2, 1), (1, 1, 0))) for _ in range(3)]
+    rho = 1.0 + 0.05 * np.cos(X + 2 * Z)
+    return P, ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, np.full_like(u, P.p0)))
+
+
+@pytest.mark.parametrize("n", [13, 21])
+def test_odd_grids_match_oracle(oracle, n):
+    P, W0 = _analytic_case(n, 40 + n)
+    p = oracle.params(P, 0.5)
+    W = W0.copy()
+    r = oracle.run(p, W, 3, 0, None, stats=False)
+    with Solver(P, cfl=0.5) as s:
+        s.upload_state(W0)
+        s.evolve_eulerian(3)
+        Wg = s.download_state()
+        _, dt_last, it = s.clock()
+    assert it == 3 and dt_last == pytest.approx(r["dt"][-1], rel=1e-13)
+    assert rel_l2(Wg, W).max() <= FIELD_TOL
+
+
 def test_plug_point_evolve_matches_eulerian_step():
     P, W0 = case(24, 0.3, 30.0, 8)
     with Solver(P, cfl=0.5) as s:
