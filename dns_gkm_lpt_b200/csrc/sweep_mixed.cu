@@ -1,4 +1,4 @@
-// Mixed-precision form of the sweeps (north-star precision pattern): WENO
+// Mixed-precision form of the sweeps (the precision pattern beside the FP64 drop-in): WENO
 // reconstruction and the gas-kinetic flux in single precision on
 // non-dimensional values, the BGK time coefficients in double (their
 // 1 - exp(-dt/tau) differences cancel), the state, the flux differences and the

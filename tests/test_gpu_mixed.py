@@ -3,7 +3,7 @@ non-dimensional FP32, time coefficients, flux differences, update and
 reductions in FP64.  Checked against the FP64 path and the reference goldens.
 
 Tolerances: field relative L2 per conserved component <= 1e-5 after 10 steps
-(the north-star error bar for the mixed form); exact properties (uniform flow,
+(the error bar of the mixed form); exact properties (uniform flow,
 conservation) as for FP64.
 """
 import numpy as np

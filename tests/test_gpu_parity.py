@@ -3,7 +3,7 @@ reference's CPU build (golden vectors) and with the CPU oracle.
 
 Tolerances (FP64 drop-in):
   * fields after 1 and 10 steps: relative L2 per conserved component <= 1e-12
-    (the north-star bar); the CUDA path rounds differently (reciprocals, FMA,
+    (the parity bar of the FP64 form); the CUDA path rounds differently (reciprocals, FMA,
     reorganised moment sums) but computes the same algorithm;
   * single-face flux: |dF| <= 1e-11 * max|F| of the face; WENO faces 1e-13 relative;
   * spline coefficients: bit-exact with the oracle (same rounding order);
