@@ -88,10 +88,9 @@ __device__ __forceinline__ double viscosity(const FieldConst& fc, double T)
     return fc.mu0 * (x * sqrt(x)) * (fc.T0 + 110.4) / (T + 110.4);   // Sutherland, src/update.cpp:277
 }
 
-// max(|u| + c) term of one cell with the reference's rounding (src/update.cpp:844-853,1041-1048)
-// |u| + c of a conserved state in FP64.  The mixed form (whose fields carry FP32 flux errors
-// anyway) takes one reciprocal of rho instead of five divisions; the FP64 drop-in keeps the
-// reference's divisions (src/update.cpp:1039-1046 via c2p), so its dt is the reference's bit for bit.
+// |u| + c of a conserved state in FP64: with one reciprocal of rho (the mixed form, whose
+// fields carry FP32 flux errors anyway), and with the reference's divisions
+// (src/update.cpp:1039-1046 via c2p), which give the FP64 form's dt bit for bit.
 __device__ __forceinline__ double wave_speed_recip(const double w[5], double gam, double gm1)
 {
     const double d = w[0], id = 1.0 / d;
@@ -479,7 +478,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                         wn[q] = __dsub_rn(wq, __dmul_rn(fc.inv_dx, s));
                         a.A[q * nt3 + ci] = wn[q];
                     }
-                    double ws = kMixed ? wave_speed_recip(wn, fc.gam, fc.gm1) : wave_speed(wn, fc.gam, fc.gm1);
+                    const double ws = kMixed ? wave_speed_recip(wn, fc.gam, fc.gm1) : wave_speed(wn, fc.gam, fc.gm1);
                     if (!isfinite(ws) || !(wn[0] > 0.0)) bad = true;
                     else wmax = ws > wmax ? ws : wmax;
                 }
