@@ -175,9 +175,13 @@ def run_reference(workers: int, warm: int, steps: int, n=REF_N, npart=REF_PART):
 def reference_arm(args, world: int):
     ncpu = os.cpu_count() or 1
     workers = max(1, min(ncpu, 96))
-    r = run_reference(workers, args.warmup, args.steps)
+    # a bounded sample: a reference step of a 64^3 cube takes ~2 s on one core, so at most 10 timed
+    # and 1 warm-up step per process keep the arm within a minute whatever --steps says
+    ref_steps, ref_warm = max(1, min(args.steps, 10)), min(args.warmup, 1)
+    r = run_reference(workers, ref_warm, ref_steps)
     sample = (f"{REF_N}^3 cube per process (same spectrum recipe, Mt {MT}, Re_lambda {RE:g}), {REF_PART} particles "
-              f"per process, {workers} concurrent processes, each timed step one reference step")
+              f"per process, {workers} concurrent processes, {ref_steps} timed reference steps each "
+              f"after {ref_warm} warm-up ({r['wall_s']:.1f} s wall)")
     line = {"impl": "reference", "metric": "Gcell-updates/s", "value": r["gcell"], "unit": "Gcell-updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
