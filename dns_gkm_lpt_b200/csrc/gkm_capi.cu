@@ -850,7 +850,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
                                 &h->pipe_comp[3]})
             CK(h, cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
     }
-    const size_t nev = 2 * (size_t)K + 2;
+    const size_t nev = 3 * (size_t)K + 2;
     while (h->pipe_ev.size() < nev) {
         cudaEvent_t e;
         CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -859,6 +859,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     cudaEvent_t ev_start = h->pipe_ev[0], ev_done_out = h->pipe_ev[1];
     cudaEvent_t* ev_in = &h->pipe_ev[2];
     cudaEvent_t* ev_out = &h->pipe_ev[2 + K];
+    cudaEvent_t* ev_head = &h->pipe_ev[2 + 2 * K];
     double* Wd = h->buf[h->parity];
     double* A = h->buf[h->parity ^ 1];
     DevClock* ck = h->clock;
@@ -891,23 +892,31 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
         return cudaSuccess;
     };
 
-    // copy-in stream: the last three interior planes first, then the chunks, each with its ghosts
+    // copy-in stream: the last three interior planes first, then per chunk its first three planes
+    // (all that the previous chunk's sweeps need of it) and the rest, each part with its ghosts
     CK(h, copy_in(n, n + 3));
     for (int c = 0; c < K; c++) {
         const int J0 = 3 + c * C, J1 = 3 + std::min((c + 1) * C, n);
         const int J1c = (J0 < n) ? std::min(J1, n) : J1;   // planes n..n+2 are already in
-        if (J1c > J0) CK(h, copy_in(J0, J1c));
+        const int Jh = std::min(J0 + 3, J1), Jhc = std::min(Jh, J1c);
+        if (Jhc > J0) CK(h, copy_in(J0, Jhc));
         if (c == 0) {
             CK(h, gkm::launch_halo_planes(Wd, fc, 0, 3, h->pipe_in));
             CK(h, gkm::launch_halo_planes(Wd, fc, n + 3, n + 6, h->pipe_in));
             h->launches += 2;
         }
-        CK(h, gkm::launch_halo_planes(Wd, fc, J0, J1, h->pipe_in));
+        CK(h, gkm::launch_halo_planes(Wd, fc, J0, Jh, h->pipe_in));
         h->launches += 1;
+        CK(h, cudaEventRecord(ev_head[c], h->pipe_in));
+        if (J1c > Jhc) CK(h, copy_in(Jhc, J1c));
+        if (J1 > Jh) {
+            CK(h, gkm::launch_halo_planes(Wd, fc, Jh, J1, h->pipe_in));
+            h->launches += 1;
+        }
         CK(h, cudaEventRecord(ev_in[c], h->pipe_in));
     }
 
-    // compute: chunk c on compute stream c % S, after the copy-in of chunk c+1
+    // compute: chunk c on compute stream c % S, after its own planes and the first three of chunk c+1
     gkm::SweepArgs a{};
     a.W = Wd;
     a.A = A;
@@ -919,7 +928,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     a.skip_clock_init = 1;
     for (int c = 0; c < K; c++) {
         cudaStream_t s = h->pipe_comp[c % S];
-        CK(h, cudaStreamWaitEvent(s, ev_in[std::min(c + 1, K - 1)], 0));
+        CK(h, cudaStreamWaitEvent(s, c + 1 < K ? ev_head[c + 1] : ev_in[c], 0));
         const int j0 = c * C, j1 = std::min((c + 1) * C, n);
         for (int d = 0; d < 3; d++) {
             gkm::SweepArgs ad = a;
