@@ -116,6 +116,7 @@ gkm_status refresh(gkm_ensemble* E, bool need_state)
         md.scratch[2] = h->scratch_extra[1] ? h->scratch_extra[1] : E->extra_scratch[2 * (size_t)m + 1];
         for (int c = 0; c < 6; c++) md.P[c] = h->P[c];
         md.np = h->np;
+        md.tmaps = h->d_tmaps;
         const long long N = h->grid.npts, M = N + h->grid.pad;
         const long long nt = h->fc.nt;
         const bool parts = h->np > 0;   // members without particles skip the spline work

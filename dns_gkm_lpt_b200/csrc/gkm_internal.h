@@ -188,6 +188,9 @@ struct MemberDev {
     double* scratch[3];
     double* P[6];        // particles y, x, z, u, v, w
     long long np;
+    // the member's tensor maps of its two state buffers for the FP64 x / y sweeps (the single
+    // cube's table: index (buffer * kSweepVariants64 + variant) * 2 + direction), or null
+    const unsigned char* tmaps;
 };
 
 struct EnsembleWork {           // prefix offsets, nm + 1 entries each, in device memory

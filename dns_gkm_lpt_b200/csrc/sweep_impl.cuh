@@ -492,6 +492,10 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
         if (tid == 0 && m > 0.0) atomicMax(&a.clock->wave[a.parity ^ 1], (unsigned long long)__double_as_longlong(m));
         if (bad) atomicOr(&a.clock->status, 1);
     }
+    if (use_tma) {   // every wait on the barrier has returned: retire it (a persistent CTA re-initialises it)
+        __syncthreads();
+        if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar_u32) : "memory");
+    }
 }
 
 template <int DIR, class T, class Tile>
@@ -520,7 +524,11 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
         const int bz = (int)(local % nseg);
         const long long t = local / nseg;
         SweepArgs a;
-        a.tmap = nullptr;
+        // FP64 x / y sweeps: the member's tensor map of the buffer read (variant 1 = 16x16 windows)
+        constexpr int kVariant = (sizeof(T) == 8 && Tile::TA == 16) ? 1 : 0;
+        a.tmap = (sizeof(T) == 8 && DIR < 2 && md.tmaps)
+                     ? md.tmaps + 128 * ((parity * kSweepVariants64 + kVariant) * 2 + DIR)
+                     : nullptr;
         a.tile_a0 = 0;
         a.seg0 = 0;
         a.skip_clock_init = 0;
