@@ -74,3 +74,30 @@ def test_null_handle_calls_fail_cleanly():
     assert L.gkm_step(None, 1) == _capi.GKM_ERR_ARG
     assert L.gkm_timestep(None, None) == _capi.GKM_ERR_ARG
     assert L.gkm_last_error(None) == b"null handle"
+
+
+def test_ensemble_and_new_entry_points_reject_bad_arguments_without_gpu():
+    L = _capi.lib()
+    h = C.c_void_p()
+    assert L.gkm_ensemble_create(None, 1, C.byref(h)) == _capi.GKM_ERR_ARG
+    cfgs = (_capi.GkmConfig * 2)()
+    for c in cfgs:
+        L.gkm_config_default(C.byref(c))
+        c.params.n, c.params.gam, c.params.den0, c.params.p0, c.params.mu0 = 16, 1.4, 1.0, 86100.0, 1.0
+    assert L.gkm_ensemble_create(cfgs, 0, C.byref(h)) == _capi.GKM_ERR_ARG
+    cfgs[1].precision = 1   # members must share the precision
+    assert L.gkm_ensemble_create(cfgs, 2, C.byref(h)) == _capi.GKM_ERR_CONFIG
+    cfgs[1].precision = 0
+    cfgs[1].device = 3      # and the device
+    assert L.gkm_ensemble_create(cfgs, 2, C.byref(h)) == _capi.GKM_ERR_CONFIG
+    assert L.gkm_ensemble_destroy(None) == _capi.GKM_ERR_ARG
+    assert L.gkm_ensemble_step(None, 1, 1) == _capi.GKM_ERR_ARG
+    assert L.gkm_ensemble_size(None) == 0
+    assert L.gkm_ensemble_member(None, 0) is None
+    assert L.gkm_ensemble_last_error(None) == b"null ensemble"
+    for fn in ("gkm_write_field", "gkm_write_particles", "gkm_write_time", "gkm_write_reinit"):
+        assert getattr(L, fn)(None, b"/dev/null") == _capi.GKM_ERR_ARG
+    assert L.gkm_particle_props(None, None) == _capi.GKM_ERR_ARG
+    assert L.gkm_particle_stats_compute(None, None) == _capi.GKM_ERR_ARG
+    assert L.gkm_set_pipeline(None, 32, 2) == _capi.GKM_ERR_ARG
+    assert L.gkm_spline_build_noalloc(None, 16, 0, 1, None, None) != _capi.GKM_OK
