@@ -24,15 +24,16 @@ __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, 
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 
 // One line: f (N points, stride fs) -> c (N+pad values, stride cs).
-// The recurrences are sequential, but their inputs are not: the loops fetch kLineBatch inputs
-// ahead (data in the forward sweeps, the forward results in the backward sweeps) so that many
-// loads are in flight per thread; the arithmetic and its order are unchanged.
-constexpr int kLineBatch = 8;
+// The recurrences are sequential, but their inputs are not: the loops fetch U inputs ahead (data
+// in the forward sweeps, the forward results in the backward sweeps) so that many loads are in
+// flight per thread; the arithmetic and its order are unchanged.  Measured: U = 8 for the
+// component-batched launches (fewer lines per component, more inputs in flight pay), U = 4 for
+// the one-component launches of large grids (their lines already fill the GPU).
+constexpr int kLineBatchBatched = 8, kLineBatchSingle = 4;
 
-template <class Src>
+template <int U, class Src>
 __device__ void line_solve(const Src& f, int N, int periodic, const SplineTables& tb, double* c, long long cs)
 {
-    constexpr int U = kLineBatch;
     if (!periodic) {
         const double c0 = f(0), cl = f(N - 1);
         double rp = 0.0;
@@ -137,6 +138,7 @@ __device__ __forceinline__ double spline_source(const double* __restrict__ W, lo
 }
 
 // pass 0: the data of source q along axis 0 (y) -> out [M0][N1][N2]; one line (i, k)
+template <int U>
 __device__ __forceinline__ void pass0_line(const double* __restrict__ W, const FieldConst& fc, const SplineGrid& g,
                                            const SplineTables& tb, int q, double* __restrict__ out, long long L)
 {
@@ -149,7 +151,7 @@ __device__ __forceinline__ void pass0_line(const double* __restrict__ W, const F
     const long long base = (long long)(i + off) * nt + (k + off);
     const long long sj = (long long)nt * nt;
     auto f = [&](int j) { return spline_source(W, nt3, fc.gm1, q, (long long)(j + off) * sj + base); };
-    line_solve(f, N, g.periodic, tb, out + L, lines);
+    line_solve<U>(f, N, g.periodic, tb, out + L, lines);
 }
 
 __global__ void spline_pass0(const double* __restrict__ W, FieldConst fc, SplineGrid g, SplineTables tb, int q,
@@ -157,10 +159,11 @@ __global__ void spline_pass0(const double* __restrict__ W, FieldConst fc, Spline
 {
     const long long lines = (long long)g.npts * g.npts;
     for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x)
-        pass0_line(W, fc, g, tb, q, out, L);
+        pass0_line<kLineBatchSingle>(W, fc, g, tb, q, out, L);
 }
 
 // pass 1: [M0][N1][N2] along axis 1 -> [M0][M1][N2]; one line (a, k)
+template <int U>
 __device__ __forceinline__ void pass1_line(const double* __restrict__ in, const SplineGrid& g, const SplineTables& tb,
                                            double* __restrict__ out, long long L)
 {
@@ -168,14 +171,14 @@ __device__ __forceinline__ void pass1_line(const double* __restrict__ in, const 
     const int a = (int)(L / N), k = (int)(L - (long long)a * N);
     const double* src = in + (long long)a * N * N + k;
     auto f = [&](int i) { return src[(long long)i * N]; };
-    line_solve(f, N, g.periodic, tb, out + (long long)a * M * N + k, N);
+    line_solve<U>(f, N, g.periodic, tb, out + (long long)a * M * N + k, N);
 }
 
 __global__ void spline_pass1(const double* __restrict__ in, SplineGrid g, SplineTables tb, double* __restrict__ out)
 {
     const long long lines = (long long)(g.npts + g.pad) * g.npts;
     for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x)
-        pass1_line(in, g, tb, out, L);
+        pass1_line<kLineBatchSingle>(in, g, tb, out, L);
 }
 
 // pass 2: [M0][M1][N2] along axis 2 -> [M0][M1][M2].  Lines are contiguous,
@@ -873,7 +876,7 @@ __global__ void ensemble_pass0_kernel(const MemberDev* __restrict__ mem, const l
         const long long local = x - off[m];
         const long long lines = (long long)md.grid.npts * md.grid.npts;
         const int q = (int)(local / lines);
-        pass0_line(md.buf[buf], md.fc, md.grid, md.tb, q + 1, md.coef[q], local - q * lines);
+        pass0_line<kLineBatchBatched>(md.buf[buf], md.fc, md.grid, md.tb, q + 1, md.coef[q], local - q * lines);
     }
 }
 
@@ -886,7 +889,7 @@ __global__ void ensemble_pass1_kernel(const MemberDev* __restrict__ mem, const l
         const long long local = x - off[m];
         const long long lines = (long long)(md.grid.npts + md.grid.pad) * md.grid.npts;
         const int q = (int)(local / lines);
-        pass1_line(md.coef[q], md.grid, md.tb, md.scratch[q], local - q * lines);
+        pass1_line<kLineBatchBatched>(md.coef[q], md.grid, md.tb, md.scratch[q], local - q * lines);
     }
 }
 
