@@ -48,7 +48,7 @@ class GkmParams(C.Structure):
 class GkmConfig(C.Structure):
     _fields_ = [("params", GkmParams), ("cfl", C.c_double), ("visc_law", C.c_int32), ("spline_mode", C.c_int32),
                 ("precision", C.c_int32), ("device", C.c_int32), ("max_particles", C.c_int64),
-                ("use_graphs", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("use_graphs", C.c_int32), ("spline_build", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 class GkmParticleStats(C.Structure):

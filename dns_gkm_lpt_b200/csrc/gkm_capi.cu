@@ -212,7 +212,8 @@ cudaError_t enqueue_splines(gkm_handle* h, const double* W)
 cudaError_t setup_batched_splines(gkm_handle* h)
 {
     const long long N = h->grid.npts, M = N + h->grid.pad;
-    if (3 * N * N > 2LL * 148 * 2048) return cudaSuccess;
+    if (h->cfg.spline_build == 1) return cudaSuccess;
+    if (h->cfg.spline_build == 0 && 3 * N * N > 2LL * 148 * 2048) return cudaSuccess;
     const size_t scratch_bytes = sizeof(double) * (size_t)(M * M * N);
     size_t free_b = 0, total_b = 0;
     cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
@@ -449,6 +450,7 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     if (cfg->visc_law < 0 || cfg->visc_law > 1 || cfg->spline_mode < 0 || cfg->spline_mode > 1) return GKM_ERR_CONFIG;
     if (cfg->precision < GKM_PREC_FP64 || cfg->precision > GKM_PREC_MIXED || cfg->max_particles < 0)
         return GKM_ERR_CONFIG;
+    if (cfg->spline_build < 0 || cfg->spline_build > 2) return GKM_ERR_CONFIG;
     const int K = (int)((5.0 - 3.0 * P.gam) / (P.gam - 1.0));   // src/FlowField.cpp:42
     if (K < 0) return GKM_ERR_CONFIG;
 

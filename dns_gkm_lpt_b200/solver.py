@@ -56,7 +56,7 @@ def _w5(W):
 
 def make_config(params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
                 max_particles: int = 0, device: int = 0, use_graphs: bool = True,
-                precision: int = 0) -> _capi.GkmConfig:
+                precision: int = 0, spline_build: int = 0) -> _capi.GkmConfig:
     L = _capi.lib()
     cfg = _capi.GkmConfig()
     L.gkm_config_default(C.byref(cfg))
@@ -69,17 +69,19 @@ def make_config(params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mod
     cfg.max_particles = max_particles
     cfg.use_graphs = 1 if use_graphs else 0
     cfg.precision = precision   # 0 FP64, 1 mixed (FP32 reconstruction + flux, FP64 state)
+    cfg.spline_build = spline_build   # 0 auto, 1 one component per launch, 2 three components per launch
     return cfg
 
 
 class Solver:
     def __init__(self, params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
                  max_particles: int = 0, device: int = 0, use_graphs: bool = True, precision: int = 0,
-                 _member_handle=None):
+                 spline_build: int = 0, _member_handle=None):
         self.L = _capi.lib()
         self._owned = _member_handle is None
         if self._owned:
-            cfg = make_config(params, cfl, visc_law, spline_mode, max_particles, device, use_graphs, precision)
+            cfg = make_config(params, cfl, visc_law, spline_mode, max_particles, device, use_graphs, precision,
+                              spline_build)
             h = C.c_void_p()
             s = self.L.gkm_create(C.byref(cfg), C.byref(h))
             if s != 0:

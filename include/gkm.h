@@ -78,7 +78,10 @@ typedef struct gkm_config {
     int32_t device;          /* CUDA device ordinal */
     int64_t max_particles;   /* capacity of the particle arrays */
     int32_t use_graphs;      /* 1: replay each step as a captured CUDA graph */
-    int32_t reserved[7];
+    int32_t spline_build;    /* velocity splines: 0 auto, 1 one component per launch, 2 each pass
+                                for all three components in one launch (two more scratch
+                                arrays; auto picks it for grids up to about 440^3); same bits */
+    int32_t reserved[6];
 } gkm_config;
 
 /* One PrintStats line (src/update.cpp:835-840), field part. */

@@ -82,21 +82,25 @@ def test_stats_match_reference(golden):
     assert st["Trms"] == pytest.approx(ref[11], rel=1e-8, abs=1e-12)
 
 
+@pytest.mark.parametrize("build", [1, 2])
 @pytest.mark.parametrize("mode", [0, 1])
-def test_spline_coefficients_bitexact_with_oracle(oracle, golden, mode):
+def test_spline_coefficients_bitexact_with_oracle(oracle, golden, mode, build):
+    """All three velocity splines, both launch forms of the build (one component per launch,
+    or each pass for all three components in one launch)."""
     g = golden["field_12"]
     P, W0 = w0_of(g)
     p = oracle.params(P, 0.5)
     start, dinv = oracle.grid(p, mode)
-    data = W0[1] / W0[0]
-    if mode == 1:
-        data = np.ascontiguousarray(data[3:-3, 3:-3, 3:-3])
-    _, ref = oracle.spline3d(data, mode, start, dinv)
-    with Solver(P, cfl=0.5, spline_mode=mode) as s:
+    with Solver(P, cfl=0.5, spline_mode=mode, spline_build=build) as s:
         s.upload_state(W0)
         s.generate_splines()
-        got = s.spline_coefs(0)
-    assert np.array_equal(got, ref)
+        got = [s.spline_coefs(c) for c in range(3)]
+    for c in range(3):
+        data = W0[1 + c] / W0[0]
+        if mode == 1:
+            data = np.ascontiguousarray(data[3:-3, 3:-3, 3:-3])
+        _, ref = oracle.spline3d(data, mode, start, dinv)
+        assert np.array_equal(got[c], ref), c
 
 
 @pytest.mark.parametrize("mode", [0, 1])
