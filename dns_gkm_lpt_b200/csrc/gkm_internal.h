@@ -79,7 +79,8 @@ struct SweepArgs {
     double dt_fixed;
     int seg_len;                    // faces per CTA along the normal
     int tile_a0;                    // first window row (x, z sweeps) of a launch over part of the j range
-    int seg0;                       // first segment (y sweep) of such a launch
+    int f0, f1;                     // y sweep over part of the j range: segments start at f0 and stop
+                                    // at f1 (f0 = f1 = 0: the whole normal range)
     int skip_clock_init;            // 1: the clock's dt and next wave slot were set before the launch
     const void* tmap;               // FP64 x / y sweeps: tensor map of W for the slab copies (else null)
 };
@@ -88,8 +89,8 @@ struct SweepArgs {
 cudaError_t sweep_prepare();
 cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s);
 // The sweep of direction dir restricted to the interior y-planes [j0, j1): window rows (x, z
-// sweeps) or normal segments (y sweep) covering them; j0 must be a multiple of the window height
-// (x, z) or of a.seg_len (y).  The cells updated are exactly those of planes [j0, j1).
+// sweeps; j0 must be a multiple of the window height) or normal segments from j0 to j1 (y sweep).
+// The cells updated are exactly those of planes [j0, j1).
 cudaError_t launch_sweep_rows(int dir, int variant, SweepArgs a, int j0, int j1, cudaStream_t s);
 cudaError_t launch_sweep_mixed_rows(int dir, int variant, SweepArgs a, int j0, int j1, cudaStream_t s);
 // Ghost cells of the ghost-layout y-planes [J0, J1) (0 <= J0 < J1 <= nt) from their periodic images

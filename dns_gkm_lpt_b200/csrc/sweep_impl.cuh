@@ -259,8 +259,8 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     const Strides st = strides<DIR>(nt);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTB + tx;
     const int b0 = bx * kTB, a0 = by * kTA;
-    const int f_begin = bz * a.seg_len;
-    const int f_end = min(f_begin + a.seg_len, n);
+    const int f_begin = a.f0 + bz * a.seg_len;
+    const int f_end = min(f_begin + a.seg_len, a.f1 > 0 ? a.f1 : n);
     const double dt = step_dt(a);
     // working units: dimensional for double, non-dimensional (dx = 1) for float
     const T dtw = kMixed ? T(dt * fc.u_s * fc.inv_dx) : T(dt);
@@ -276,7 +276,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
         a.clock->wave[a.parity ^ 1] = 0ull;   // the z sweep of this step reduces into it
         a.clock->dt = dt;
     }
-    if (f_begin >= n) return;
+    if (f_begin >= f_end) return;
 
     // FP64 x and y sweeps with a tensor map: one thread moves each new slab (5 components of the
     // window, a box of the (k, i, j, q) tensor whose smem image is the slot's [q][a][b] layout)
@@ -502,7 +502,7 @@ template <int DIR, class T, class Tile>
 __global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    sweep_block<DIR, T, Tile>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z + a.seg0, smem_raw);
+    sweep_block<DIR, T, Tile>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
 }
 
 // Persistent form for an ensemble: a fixed grid of CTAs walks the flattened
@@ -530,7 +530,8 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
                      ? md.tmaps + 128 * ((parity * kSweepVariants64 + kVariant) * 2 + DIR)
                      : nullptr;
         a.tile_a0 = 0;
-        a.seg0 = 0;
+        a.f0 = 0;
+        a.f1 = 0;
         a.skip_clock_init = 0;
         a.W = md.buf[parity];
         a.A = md.buf[parity ^ 1];
@@ -554,9 +555,10 @@ cudaError_t launch_sweep_rows_t(int dir, SweepArgs a, int j0, int j1, cudaStream
     const size_t smem = sweep_detail::sweep_smem_bytes<T, Tile>();
     const dim3 block(Tile::TB, Tile::TA);
     if (dir == 1) {
-        if (j0 % a.seg_len) return cudaErrorInvalidValue;
-        a.seg0 = j0 / a.seg_len;
-        const dim3 grid(gb, (n + Tile::TA - 1) / Tile::TA, (j1 + a.seg_len - 1) / a.seg_len - a.seg0);
+        if (a.seg_len < 1) return cudaErrorInvalidValue;
+        a.f0 = j0;
+        a.f1 = j1;
+        const dim3 grid(gb, (n + Tile::TA - 1) / Tile::TA, (j1 - j0 + a.seg_len - 1) / a.seg_len);
         sweep_kernel<1, T, Tile><<<grid, block, smem, s>>>(a);
         return cudaGetLastError();
     }

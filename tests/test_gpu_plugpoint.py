@@ -58,3 +58,24 @@ def test_pipelined_plug_point_matches_resident_step(n, prec):
         s.evolve(Wr, dt)
     assert rel_l2(Wc, Wr).max() <= 1e-13
     assert _ghosts_are_periodic(Wc)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_pipeline_stream_counts_are_bitwise_identical(prec):
+    """One, two and three compute streams launch the same sweeps on the same planes, so
+    their results agree bit for bit; 16-plane chunks at 64^3 give four chunks, so chunks on
+    different streams really overlap."""
+    n = 64
+    P, W0 = case(n, 0.3, 40.0, 77)
+    out = {}
+    with Solver(P, cfl=0.5, precision=prec) as s:
+        s.upload_state(W0)
+        dt = s.timestep()
+        for streams in (1, 2, 3):
+            s.set_pipeline(16, streams)
+            Wp = torch.from_numpy(W0.copy()).pin_memory()
+            s.evolve(Wp.numpy(), dt)
+            out[streams] = Wp.numpy().copy()
+    for streams in (2, 3):
+        assert np.array_equal(out[streams], out[1]), streams
+    assert _ghosts_are_periodic(out[1])
