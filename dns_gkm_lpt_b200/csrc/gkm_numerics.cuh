@@ -395,8 +395,11 @@ struct FaceInput {
     GKM_HD T DW(int v, int q) const { return DW_[v][q]; }
 };
 
+// The flux with the reference's moment algebra: one MCal (25 triple products
+// and their sums) per table, weight and slope vector.  The operation counter
+// instantiates this form; the kernels run gks_flux_tau below.
 template <class T, class Prov>
-GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[5])
+GKM_HD void gks_flux_mcal(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[5])
 {
     const int K = ph.K;
     T denl, Ul[3], Pl, denr, Ur[3], Pr;
@@ -542,6 +545,296 @@ GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[
     axpy5<T>(Facc, p0 * dene, M);
 #pragma unroll
     for (int q = 0; q < 5; q++) F[q] = Facc[q];
+}
+
+#if GKM_SHARED_YZ
+// ------------------------------------------------ moment functionals ----
+// Every moment the flux takes is <u^k psi_i P>_N for a table N (full or half
+// space) and a polynomial P built from slope vectors: P = psi.a, or
+// G = u (psi.a_n) + v (psi.a_y) + w (psi.a_z).  Writing P = sum_p u^p Q_p(v, w, xi^2),
+//   <u^k psi_i P>_N = sum_p N[p + k] tau_i(Q_p)          (i = 0, 2, 3)
+//   <u^k psi_1 P>_N = sum_p N[p + k + 1] tau_0(Q_p)
+//   <u^k psi_4 P>_N = sum_p (N[p + k + 2] tau_0(Q_p) / 2 + N[p + k] tau_4(Q_p))
+// with the tangential functionals tau_0 = <Q>, tau_2 = <v Q>, tau_3 = <w Q>,
+// tau_4 = <(v^2 + w^2 + xi^2) Q> / 2.  They involve the tangential tables only,
+// so one set serves the full and the half-space table and the weights u^0 and
+// u^1: a contraction costs 24 multiply-adds where MCal forms 25 triple
+// products and their sums again.  Same moments, summed in another order.
+template <class T>
+struct Tau {
+    T c0[4], cv[4], cw[4], c4[4];   // tau_0, tau_2, tau_3, tau_4 of Q_0 .. Q_3
+};
+
+template <bool ADD, class T>
+GKM_HD void put(T& x, T v)
+{
+    if constexpr (ADD) x += v;
+    else x = v;
+}
+
+// mu(q, r, s) = <v^q w^r xi^(2s)>
+template <int Q, int R, int S, class T>
+GKM_HD T mu(const Moments<T>& M)
+{
+    static_assert(Q + R <= 5 && S <= 2, "tangential moment beyond the tables");
+    if constexpr (S == 0) return M.YZ[yz(Q, R)];
+    else if constexpr (S == 1) return M.YZ[yz(Q, R)] * M.Ie2;
+    else return M.YZ[yz(Q, R)] * M.Ie4;
+}
+
+// <v^q w^r xi^(2s) R(a)>, R(a) = a0 + a2 v + a3 w + (a4/2)(v^2 + w^2 + xi^2) the u-free part of psi.a
+template <int Q, int R, int S, class T>
+GKM_HD T rho_moment(const T a[5], T h4, const Moments<T>& M)
+{
+    return a[0] * mu<Q, R, S>(M) + a[2] * mu<Q + 1, R, S>(M) + a[3] * mu<Q, R + 1, S>(M) +
+           h4 * (mu<Q + 2, R, S>(M) + mu<Q, R + 2, S>(M) + mu<Q, R, S + 1>(M));
+}
+
+// functionals of Q = v^q w^r R(a) into entry p
+template <bool ADD, int Q, int R, int P, class T>
+GKM_HD void tau_R(Tau<T>& t, const T a[5], T h4, const Moments<T>& M)
+{
+    put<ADD>(t.c0[P], rho_moment<Q, R, 0>(a, h4, M));
+    put<ADD>(t.cv[P], rho_moment<Q + 1, R, 0>(a, h4, M));
+    put<ADD>(t.cw[P], rho_moment<Q, R + 1, 0>(a, h4, M));
+    put<ADD>(t.c4[P], T(0.5) * (rho_moment<Q + 2, R, 0>(a, h4, M) + rho_moment<Q, R + 2, 0>(a, h4, M) +
+                                rho_moment<Q, R, 1>(a, h4, M)));
+}
+
+// functionals of Q = c v^q w^r into entry p
+template <bool ADD, int Q, int R, int P, class T>
+GKM_HD void tau_mono(Tau<T>& t, T c, const Moments<T>& M)
+{
+    put<ADD>(t.c0[P], c * mu<Q, R, 0>(M));
+    put<ADD>(t.cv[P], c * mu<Q + 1, R, 0>(M));
+    put<ADD>(t.cw[P], c * mu<Q, R + 1, 0>(M));
+    put<ADD>(t.c4[P], (T(0.5) * c) * (mu<Q + 2, R, 0>(M) + mu<Q, R + 2, 0>(M) + mu<Q, R, 1>(M)));
+}
+
+// functionals of psi.a: Q_0 = R(a), Q_1 = a1, Q_2 = a4/2
+template <class T>
+GKM_HD void tau_psi(Tau<T>& t, const T a[5], const Moments<T>& M)
+{
+    const T h4 = T(0.5) * a[4];
+    tau_R<false, 0, 0, 0>(t, a, h4, M);
+    tau_mono<false, 0, 0, 1>(t, a[1], M);
+    tau_mono<false, 0, 0, 2>(t, h4, M);
+}
+
+// out_i = <u^k psi_i P>_N, P = sum_{p = P0..P1} u^p Q_p
+template <int K, int P0, int P1, class T>
+GKM_HD void contract(T out[5], const T* N, const Tau<T>& t)
+{
+    static_assert(P1 + K + 2 <= 6, "normal moment beyond the table");
+    T o0 = N[P0 + K] * t.c0[P0];
+    T o1 = N[P0 + K + 1] * t.c0[P0];
+    T o2 = N[P0 + K] * t.cv[P0];
+    T o3 = N[P0 + K] * t.cw[P0];
+    T o4 = N[P0 + K] * t.c4[P0] + T(0.5) * N[P0 + K + 2] * t.c0[P0];
+#pragma unroll
+    for (int p = P0 + 1; p <= P1; p++) {
+        o0 += N[p + K] * t.c0[p];
+        o1 += N[p + K + 1] * t.c0[p];
+        o2 += N[p + K] * t.cv[p];
+        o3 += N[p + K] * t.cw[p];
+        o4 += N[p + K] * t.c4[p] + T(0.5) * N[p + K + 2] * t.c0[p];
+    }
+    out[0] = o0;
+    out[1] = o1;
+    out[2] = o2;
+    out[3] = o3;
+    out[4] = o4;
+}
+
+// The flux of gks_flux_mcal with the moment functionals above: the same
+// moments of the same slope vectors (src/GKMflux.cpp:11-229), grouped per
+// polynomial instead of per MCal call.
+template <class T, class Prov>
+GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[5])
+{
+    const int K = ph.K;
+    T denl, Ul[3], Pl, denr, Ur[3], Pr;
+    {
+        T wl[5], wr[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            wl[q] = in.Wl(q);
+            wr[q] = in.Wr(q);
+        }
+        c2p<T>(wl, ph.gm1, denl, Ul, Pl);
+        c2p<T>(wr, ph.gm1, denr, Ur, Pr);
+    }
+    T laml = T(0.5) * denl / Pl;
+    T lamr = T(0.5) * denr / Pr;
+
+    // collision time with the pressure-jump correction, src/GKMflux.cpp:156-157
+    T ql = denl / laml, qr = denr / lamr;
+    const TimeCoefs<wide_t<T>> tc = time_coefs<wide_t<T>, (sizeof(T) < sizeof(wide_t<T>))>(
+        wide_t<T>(tau0) + wide_t<T>(dt) * wide_t<T>(fabs(ql - qr) / fabs(ql + qr)), wide_t<T>(dt));
+    const T gm1 = T(tc.gm1), gm2 = T(tc.gm2), gm3 = T(tc.gm3), gm4 = T(tc.gm4), gm5 = T(tc.gm5);
+    const T p0 = T(tc.p0), p1 = T(tc.p1), p2 = T(tc.p2), p3 = T(tc.p3), p4 = T(tc.p4), p5 = T(tc.p5);
+
+    T We[5] = {0, 0, 0, 0, 0};      // equilibrium state at the face, src/GKMflux.cpp:73-77
+    T by_[5] = {0, 0, 0, 0, 0}, bz_[5] = {0, 0, 0, 0, 0};
+    T Bacc[5] = {0, 0, 0, 0, 0};   // B_ * dene, without the gm1/gm3 terms
+    T Facc[5] = {0, 0, 0, 0, 0};
+    T M[5];
+
+    const T cB = gm4 + gm5;
+    // ---------------- one side (l: positive half with left state, r: negative half with right state)
+#if GKM_UNROLL_SIDES
+#pragma unroll
+#else
+#pragma unroll 1
+#endif
+    for (int side = 0; side < 2; side++) {
+        const T den = side == 0 ? denl : denr;
+        const T* Us = side == 0 ? Ul : Ur;
+        const T lam = side == 0 ? laml : lamr;
+        Moments<T> S;
+        build_moments<T>(S, Us, lam, K, side == 0 ? +1 : -1);
+        SlopeState<T> ss = slope_state<T>(Us, lam, K);
+        T iden = T(1) / den;
+        mcal0<0, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2);
+        axpy5<T>(We, den, M);
+        // G = u (psi.a_n) + v (psi.a_y) + w (psi.a_z):
+        //   Q_0 = v R(a_y) + w R(a_z), Q_1 = R(a_n) + a1y v + a1z w,
+        //   Q_2 = a1n + (a4y/2) v + (a4z/2) w, Q_3 = a4n/2
+        Tau<T> tg, tp;
+        T b[5], a[5];
+        // normal slope
+#pragma unroll
+        for (int q = 0; q < 5; q++) b[q] = in.DW(0 + side, q) * iden;
+        slope_solve<T>(b, ss, a);
+        {
+            const T h4 = T(0.5) * a[4];
+            tau_R<false, 0, 0, 1>(tg, a, h4, S);
+            tau_mono<false, 0, 0, 2>(tg, a[1], S);
+            tau_mono<false, 0, 0, 3>(tg, h4, S);
+        }
+        // first tangential slope: <psi (psi.a_y)>_H feeds the equilibrium's y slope
+#pragma unroll
+        for (int q = 0; q < 5; q++) b[q] = in.DW(2 + side, q) * iden;
+        slope_solve<T>(b, ss, a);
+        {
+            const T h4 = T(0.5) * a[4];
+            tau_psi<T>(tp, a, S);
+            contract<0, 0, 2>(M, S.H, tp);
+            axpy5<T>(by_, T(1), M);
+            tau_R<false, 1, 0, 0>(tg, a, h4, S);
+            tau_mono<true, 1, 0, 1>(tg, a[1], S);
+            tau_mono<true, 1, 0, 2>(tg, h4, S);
+        }
+        // second tangential slope
+#pragma unroll
+        for (int q = 0; q < 5; q++) b[q] = in.DW(4 + side, q) * iden;
+        slope_solve<T>(b, ss, a);
+        {
+            const T h4 = T(0.5) * a[4];
+            tau_psi<T>(tp, a, S);
+            contract<0, 0, 2>(M, S.H, tp);
+            axpy5<T>(bz_, T(1), M);
+            tau_R<true, 0, 1, 0>(tg, a, h4, S);
+            tau_mono<true, 0, 1, 1>(tg, a[1], S);
+            tau_mono<true, 0, 1, 2>(tg, h4, S);
+        }
+        // -<psi G>_X is the right-hand side of this side's time slope, src/GKMflux.cpp:145-151
+        contract<0, 0, 3>(M, S.X, tg);
+#pragma unroll
+        for (int q = 0; q < 5; q++) b[q] = -M[q];
+        contract<0, 0, 3>(M, S.H, tg);
+        axpy5<T>(Bacc, cB * den, M);
+        contract<1, 0, 3>(M, S.H, tg);
+        axpy5<T>(Facc, p4 * den, M);
+        // time slope of this side
+        slope_solve<T>(b, ss, a);
+        tau_psi<T>(tp, a, S);
+        contract<0, 0, 2>(M, S.H, tp);
+        axpy5<T>(Bacc, gm5 * den, M);
+        contract<1, 0, 2>(M, S.H, tp);
+        axpy5<T>(Facc, p5 * den, M);
+        // free transport of the initial half-Maxwellian
+        mcal0<1, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2);
+        axpy5<T>(Facc, p3 * den, M);
+    }
+
+    // ---------------- equilibrium part
+    T dene, Ue[3], Pe;
+    c2p<T>(We, ph.gm1, dene, Ue, Pe);
+    T lame = T(0.5) * dene / Pe;
+    Moments<T> E;
+    build_moments<T>(E, Ue, lame, K, +1);
+    // the negative half space of the equilibrium: full table minus the positive half
+    T H2[7];
+#pragma unroll
+    for (int i = 0; i < 7; i++) H2[i] = E.X[i] - E.H[i];
+    SlopeState<T> se = slope_state<T>(Ue, lame, K);
+    Tau<T> tp;
+    T b[5], a[5];
+    const T idx2 = T(2) / (dene * dx);
+    // normal equilibrium slopes from the cell averages, src/GKMflux.cpp:115-116
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (We[q] - in.WL(q)) * idx2;
+    slope_solve<T>(b, se, a);
+    tau_psi<T>(tp, a, E);
+    contract<1, 0, 2>(M, E.H, tp);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    contract<2, 0, 2>(M, E.H, tp);
+    axpy5<T>(Facc, p2 * dene, M);
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (in.WR(q) - We[q]) * idx2;
+    slope_solve<T>(b, se, a);
+    tau_psi<T>(tp, a, E);
+    contract<1, 0, 2>(M, H2, tp);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    contract<2, 0, 2>(M, H2, tp);
+    axpy5<T>(Facc, p2 * dene, M);
+    // tangential equilibrium slopes: G_E = v (psi.a_y) + w (psi.a_z),
+    //   Q_0 = v R(a_y) + w R(a_z), Q_1 = a1y v + a1z w, Q_2 = (a4y/2) v + (a4z/2) w
+    slope_solve<T>(by_, se, a);
+    {
+        const T h4 = T(0.5) * a[4];
+        tau_R<false, 1, 0, 0>(tp, a, h4, E);
+        tau_mono<false, 1, 0, 1>(tp, a[1], E);
+        tau_mono<false, 1, 0, 2>(tp, h4, E);
+    }
+    slope_solve<T>(bz_, se, a);
+    {
+        const T h4 = T(0.5) * a[4];
+        tau_R<true, 0, 1, 0>(tp, a, h4, E);
+        tau_mono<true, 0, 1, 1>(tp, a[1], E);
+        tau_mono<true, 0, 1, 2>(tp, h4, E);
+    }
+    contract<0, 0, 2>(M, E.X, tp);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    contract<1, 0, 2>(M, E.X, tp);
+    axpy5<T>(Facc, p2 * dene, M);
+    // time derivative of the equilibrium, src/GKMflux.cpp:183-191
+    mcal0<0, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
+    T idene = T(1) / dene;
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (gm1 * dene * M[q] + Bacc[q] + gm3 * We[q]) * idene;
+    slope_solve<T>(b, se, a);
+    tau_psi<T>(tp, a, E);
+    contract<1, 0, 2>(M, E.X, tp);
+    axpy5<T>(Facc, p1 * dene, M);
+    mcal0<1, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
+    axpy5<T>(Facc, p0 * dene, M);
+#pragma unroll
+    for (int q = 0; q < 5; q++) F[q] = Facc[q];
+}
+#endif
+
+// The flux the kernels run: the functional form where the tangential product
+// table exists (GKM_SHARED_YZ), else the reference's MCal form.
+template <class T, class Prov>
+GKM_HD void gks_flux(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[5])
+{
+#if GKM_SHARED_YZ
+    gks_flux_tau<T>(in, tau0, dt, dx, ph, F);
+#else
+    gks_flux_mcal<T>(in, tau0, dt, dx, ph, F);
+#endif
 }
 
 }  // namespace gkm
