@@ -29,6 +29,14 @@
 #define GKM_HD inline
 #endif
 
+// GKM_REFERENCE_FORM 1 keeps the reference's arithmetic in the shared helpers
+// (two divisions per WENO scalar, the divisions of temperature and face energy)
+// and its MCal moment algebra; the operation counter compiles that form.  The
+// kernels (0) form each reciprocal once and fold the moments.
+#ifndef GKM_REFERENCE_FORM
+#define GKM_REFERENCE_FORM 0
+#endif
+
 // Code shape of the flux: both half-Maxwellian sides unrolled (one copy of the
 // side code per side) or one loop body.
 #ifndef GKM_UNROLL_SIDES
@@ -98,18 +106,31 @@ GKM_HD void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
         fr = (a0 * P0n + a1 * P1n + a2 * P2n + a3 * P3n) / (a0 + a1 + a2 + a3);
         return;
     }
+    T Nl, Dl, Nr, Dr;
     {
         T e0 = eps + I0p, e1 = eps + I1p, e2 = eps + I2p, e3 = eps + I3p;
         T p01 = e0 * e1, p23 = e2 * e3;
         T n0 = e1 * p23, n1 = T(9) * e0 * p23, n2 = T(9) * p01 * e3, n3 = p01 * e2;
-        fl = (n0 * P0p + n1 * P1p + n2 * P2p + n3 * P3p) / (n0 + n1 + n2 + n3);
+        Nl = n0 * P0p + n1 * P1p + n2 * P2p + n3 * P3p;
+        Dl = n0 + n1 + n2 + n3;
     }
     {
         T e0 = eps + I0n, e1 = eps + I1n, e2 = eps + I2n, e3 = eps + I3n;
         T p01 = e0 * e1, p23 = e2 * e3;
         T n0 = e1 * p23, n1 = T(9) * e0 * p23, n2 = T(9) * p01 * e3, n3 = p01 * e2;
-        fr = (n0 * P0n + n1 * P1n + n2 * P2n + n3 * P3n) / (n0 + n1 + n2 + n3);
+        Nr = n0 * P0n + n1 * P1n + n2 * P2n + n3 * P3n;
+        Dr = n0 + n1 + n2 + n3;
     }
+#if GKM_REFERENCE_FORM
+    fl = Nl / Dl;
+    fr = Nr / Dr;
+#else
+    // both sides with one division: D ranges from 4 eps^3 (flat stencil) to (IS_max)^3, so
+    // Dl Dr stays inside the double range for any physical state
+    const T inv = T(1) / (Dl * Dr);
+    fl = Nl * (Dr * inv);
+    fr = Nr * (Dl * inv);
+#endif
 }
 
 // temperature of a conserved state, src/update.cpp:615-620
@@ -117,14 +138,22 @@ template <class T>
 GKM_HD T temperature(T r, T m1, T m2, T m3, T E, const Phys<T>& ph)
 {
     T ir = T(1) / r;
+#if GKM_REFERENCE_FORM
     return ph.gm1 * (E * ir - T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) * ir * ir) / ph.Rg;
+#else
+    return (E * ir - T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) * ir * ir) * (ph.gm1 / ph.Rg);
+#endif
 }
 
 // face energy from reconstructed rho, momentum and temperature, src/update.cpp:673-674
 template <class T>
 GKM_HD T face_energy(T r, T m1, T m2, T m3, T Tf, const Phys<T>& ph)
 {
+#if GKM_REFERENCE_FORM
     return r * ph.Rg * Tf / ph.gm1 + T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) / r;
+#else
+    return r * Tf * (ph.Rg / ph.gm1) + T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) / r;
+#endif
 }
 
 // ------------------------------------------------------ moment tables ----
@@ -138,7 +167,7 @@ GKM_HD T face_energy(T r, T m1, T m2, T m3, T Tf, const Phys<T>& ph)
 // with two multiplications as the reference's MCal does; the operation counter
 // uses that to count the reference formulation.)
 #ifndef GKM_SHARED_YZ
-#define GKM_SHARED_YZ 1
+#define GKM_SHARED_YZ (!GKM_REFERENCE_FORM)
 #endif
 constexpr int kYZ = 21;
 GKM_HD constexpr int yz(int b, int c) { return 6 * c - c * (c - 1) / 2 + b; }
@@ -173,6 +202,27 @@ template <>
 GKM_HD double sqrt_t<double>(double x) { return sqrt(x); }
 template <>
 GKM_HD float sqrt_t<float>(float x) { return sqrtf(x); }
+// 1 / sqrt(x): the device's reciprocal square root (within 1 ulp), on the host 1 / sqrt
+template <class T>
+GKM_HD T rsqrt_t(T x);
+template <>
+GKM_HD double rsqrt_t<double>(double x)
+{
+#ifdef __CUDA_ARCH__
+    return rsqrt(x);
+#else
+    return 1.0 / sqrt(x);
+#endif
+}
+template <>
+GKM_HD float rsqrt_t<float>(float x)
+{
+#ifdef __CUDA_ARCH__
+    return rsqrtf(x);
+#else
+    return 1.0f / sqrtf(x);
+#endif
+}
 
 // half: +1 positive-u half space (erfc(-sqrt(lam) u)/2), -1 negative half
 template <class T>
@@ -646,6 +696,72 @@ GKM_HD void contract(T out[5], const T* N, const Tau<T>& t)
     out[4] = o4;
 }
 
+// Primitive values of a state with the reciprocals the flux reuses: 1/rho,
+// lam = rho / (2 p) and 1 / (2 lam) = p / rho from one reciprocal of p.
+template <class T>
+struct Prim {
+    T den, ir, U[3], P, lam, inv2lam;
+};
+
+template <class T>
+GKM_HD Prim<T> prim(const T W[5], T gm1)
+{
+    Prim<T> s;
+    s.den = W[0];
+    s.ir = T(1) / s.den;
+    s.U[0] = W[1] * s.ir;
+    s.U[1] = W[2] * s.ir;
+    s.U[2] = W[3] * s.ir;
+    s.P = (s.den * gm1) * (W[4] * s.ir - T(0.5) * (s.U[0] * s.U[0] + s.U[1] * s.U[1] + s.U[2] * s.U[2]));
+    s.lam = T(0.5) * s.den * (T(1) / s.P);
+    s.inv2lam = s.P * s.ir;
+    return s;
+}
+
+// moment tables of a state (build_moments) with sqrt(lam) and 1/sqrt(lam pi) from one
+// reciprocal square root
+template <class T>
+GKM_HD void build_moments_prim(Moments<T>& M, const Prim<T>& st, int K, int half)
+{
+    const T inv2lam = st.inv2lam, U0 = st.U[0];
+    M.Ie2 = T(K) * inv2lam;
+    M.Ie4 = T(3 * K + K * (K - 1)) * inv2lam * inv2lam;
+    const T isl = rsqrt_t<T>(st.lam);
+    const T sl = st.lam * isl;
+    const T g = T(0.28209479177387814347) * exp_t<T>(-st.lam * U0 * U0) * isl;   // 1 / (2 sqrt(pi))
+    if (half > 0) {
+        M.H[0] = T(0.5) * erfc_t<T>(-sl * U0);
+        M.H[1] = U0 * M.H[0] + g;
+    } else {
+        M.H[0] = T(0.5) * erfc_t<T>(sl * U0);
+        M.H[1] = U0 * M.H[0] - g;
+    }
+#pragma unroll
+    for (int i = 2; i < 7; i++) M.H[i] = U0 * M.H[i - 1] + M.H[i - 2] * (T(i - 1) * inv2lam);
+    full_table<T, 7>(M.X, U0, inv2lam);
+    T Y[6], Z[6];
+    full_table<T, 6>(Y, st.U[1], inv2lam);
+    full_table<T, 6>(Z, st.U[2], inv2lam);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+#pragma unroll
+        for (int b = 0; b + c < 6; b++) M.YZ[yz(b, c)] = Y[b] * Z[c];
+}
+
+// slope_state without divisions: (K+3)/(2 lam) = (K+3) inv2lam; iK3 = 1/(K+3)
+template <class T>
+GKM_HD SlopeState<T> slope_state_prim(const Prim<T>& st, T iK3, int K)
+{
+    SlopeState<T> s;
+    s.U[0] = st.U[0];
+    s.U[1] = st.U[1];
+    s.U[2] = st.U[2];
+    s.lam2 = T(2) * st.lam;
+    s.usqc = st.U[0] * st.U[0] + st.U[1] * st.U[1] + st.U[2] * st.U[2] + T(K + 3) * st.inv2lam;
+    s.a4fac = T(1.0 / kPrandtl) * (T(4) * st.lam * st.lam) * iK3;
+    return s;
+}
+
 // The flux of gks_flux_mcal with the moment functionals above: the same
 // moments of the same slope vectors (src/GKMflux.cpp:11-229), grouped per
 // polynomial instead of per MCal call.
@@ -653,7 +769,8 @@ template <class T, class Prov>
 GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, T F[5])
 {
     const int K = ph.K;
-    T denl, Ul[3], Pl, denr, Ur[3], Pr;
+    const T iK3 = T(1) / T(K + 3);
+    Prim<T> stl, str;
     {
         T wl[5], wr[5];
 #pragma unroll
@@ -661,16 +778,14 @@ GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, 
             wl[q] = in.Wl(q);
             wr[q] = in.Wr(q);
         }
-        c2p<T>(wl, ph.gm1, denl, Ul, Pl);
-        c2p<T>(wr, ph.gm1, denr, Ur, Pr);
+        stl = prim<T>(wl, ph.gm1);
+        str = prim<T>(wr, ph.gm1);
     }
-    T laml = T(0.5) * denl / Pl;
-    T lamr = T(0.5) * denr / Pr;
 
-    // collision time with the pressure-jump correction, src/GKMflux.cpp:156-157
-    T ql = denl / laml, qr = denr / lamr;
+    // collision time with the pressure-jump correction, src/GKMflux.cpp:156-157:
+    // |rho_l/lam_l - rho_r/lam_r| / |rho_l/lam_l + rho_r/lam_r| with rho/lam = 2 p
     const TimeCoefs<wide_t<T>> tc = time_coefs<wide_t<T>, (sizeof(T) < sizeof(wide_t<T>))>(
-        wide_t<T>(tau0) + wide_t<T>(dt) * wide_t<T>(fabs(ql - qr) / fabs(ql + qr)), wide_t<T>(dt));
+        wide_t<T>(tau0) + wide_t<T>(dt) * wide_t<T>(fabs(stl.P - str.P) / fabs(stl.P + str.P)), wide_t<T>(dt));
     const T gm1 = T(tc.gm1), gm2 = T(tc.gm2), gm3 = T(tc.gm3), gm4 = T(tc.gm4), gm5 = T(tc.gm5);
     const T p0 = T(tc.p0), p1 = T(tc.p1), p2 = T(tc.p2), p3 = T(tc.p3), p4 = T(tc.p4), p5 = T(tc.p5);
 
@@ -688,13 +803,12 @@ GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, 
 #pragma unroll 1
 #endif
     for (int side = 0; side < 2; side++) {
-        const T den = side == 0 ? denl : denr;
-        const T* Us = side == 0 ? Ul : Ur;
-        const T lam = side == 0 ? laml : lamr;
+        const Prim<T>& st = side == 0 ? stl : str;
+        const T den = st.den;
         Moments<T> S;
-        build_moments<T>(S, Us, lam, K, side == 0 ? +1 : -1);
-        SlopeState<T> ss = slope_state<T>(Us, lam, K);
-        T iden = T(1) / den;
+        build_moments_prim<T>(S, st, K, side == 0 ? +1 : -1);
+        SlopeState<T> ss = slope_state_prim<T>(st, iK3, K);
+        const T iden = st.ir;
         mcal0<0, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2);
         axpy5<T>(We, den, M);
         // G = u (psi.a_n) + v (psi.a_y) + w (psi.a_z):
@@ -759,19 +873,18 @@ GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, 
     }
 
     // ---------------- equilibrium part
-    T dene, Ue[3], Pe;
-    c2p<T>(We, ph.gm1, dene, Ue, Pe);
-    T lame = T(0.5) * dene / Pe;
+    const Prim<T> ste = prim<T>(We, ph.gm1);
+    const T dene = ste.den;
     Moments<T> E;
-    build_moments<T>(E, Ue, lame, K, +1);
+    build_moments_prim<T>(E, ste, K, +1);
     // the negative half space of the equilibrium: full table minus the positive half
     T H2[7];
 #pragma unroll
     for (int i = 0; i < 7; i++) H2[i] = E.X[i] - E.H[i];
-    SlopeState<T> se = slope_state<T>(Ue, lame, K);
+    SlopeState<T> se = slope_state_prim<T>(ste, iK3, K);
     Tau<T> tp;
     T b[5], a[5];
-    const T idx2 = T(2) / (dene * dx);
+    const T idx2 = (T(2) / dx) * ste.ir;
     // normal equilibrium slopes from the cell averages, src/GKMflux.cpp:115-116
 #pragma unroll
     for (int q = 0; q < 5; q++) b[q] = (We[q] - in.WL(q)) * idx2;
@@ -811,7 +924,7 @@ GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, 
     axpy5<T>(Facc, p2 * dene, M);
     // time derivative of the equilibrium, src/GKMflux.cpp:183-191
     mcal0<0, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
-    T idene = T(1) / dene;
+    const T idene = ste.ir;
 #pragma unroll
     for (int q = 0; q < 5; q++) b[q] = (gm1 * dene * M[q] + Bacc[q] + gm3 * We[q]) * idene;
     slope_solve<T>(b, se, a);

@@ -1,9 +1,10 @@
 // Algorithmic operation count of one cell update, taken from the device
 // numerics themselves: gkm_numerics.cuh is instantiated on the host with a
 // scalar type that counts every arithmetic operation it performs, in the
-// reference's formulation of the moments (GKM_SHARED_YZ 0) and with one
-// reconstruction per face.  The count is the numerator of the FP64 roofline
-// reported by bench.py, so it stays fixed when the kernels get cheaper.
+// reference's formulation (GKM_REFERENCE_FORM 1: its moment algebra and its
+// divisions) and with one reconstruction per face.  The count is the numerator
+// of the FP64 roofline reported by bench.py, so it stays fixed when the kernels
+// get cheaper.
 //
 // Per face (one reconstruction per face, as the sweep kernels do):
 //   temperature of the cell entering the stencil window  1x
@@ -43,9 +44,9 @@ inline Num fabs(Num a) { return Num(std::fabs(a.v)); }
 inline Num fmax(Num a, Num b) { g_cnt.cmp++; return Num(std::fmax(a.v, b.v)); }
 
 // count the gas-kinetic moments as the reference's MCal forms them
-// (src/GKMflux.cpp:238-278: two multiplications per triple product); the
-// kernels share the Y*Z products and execute fewer
-#define GKM_SHARED_YZ 0
+// (src/GKMflux.cpp:238-278: two multiplications per triple product) and its
+// divisions; the kernels fold the moments, form reciprocals once and execute fewer
+#define GKM_REFERENCE_FORM 1
 #include "gkm_numerics.cuh"
 
 namespace gkm {

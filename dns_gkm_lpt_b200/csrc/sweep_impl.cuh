@@ -81,11 +81,13 @@ struct SmemFace {
     }
 };
 
-__device__ __forceinline__ double viscosity(const FieldConst& fc, double T)
+// tau0 = mu(T) / p of a cell (src/update.cpp:276-278) with one division: Sutherland
+// mu0 x^(3/2) (T0 + 110.4) / (T + 110.4), x = T / T0, or the power law mu0 x^0.76
+__device__ __forceinline__ double collision_time(const FieldConst& fc, double T, double p)
 {
-    double x = T / fc.T0;
-    if (fc.visc == 1) return fc.mu0 * pow(x, 0.76);
-    return fc.mu0 * (x * sqrt(x)) * (fc.T0 + 110.4) / (T + 110.4);   // Sutherland, src/update.cpp:277
+    const double x = T * fc.inv_T0;
+    if (fc.visc == 1) return fc.mu0 * pow(x, 0.76) / p;
+    return fc.mu0 * (x * sqrt(x)) * (fc.T0 + 110.4) / ((T + 110.4) * p);
 }
 
 // |u| + c of a conserved state in FP64: with one reciprocal of rho (the mixed form, whose
@@ -429,13 +431,13 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 const float u = wl[kWC + cc] * id, v = wl[2 * kWC + cc] * id, w = wl[3 * kWC + cc] * id;
                 const float p = (d * float(fc.gm1)) * (wl[4 * kWC + cc] * id - 0.5f * (u * u + v * v + w * w));
                 const double Tk = (double)(p * id) * fc.T0;
-                tau0 = T(viscosity(fc, Tk) / ((double)p * fc.p0) * fc.u_s * fc.inv_dx);
+                tau0 = T(collision_time(fc, Tk, (double)p * fc.p0) * fc.u_s * fc.inv_dx);
             } else {
                 double d = wl[cc], id = 1.0 / d;
                 double u = wl[kWC + cc] * id, v = wl[2 * kWC + cc] * id, w = wl[3 * kWC + cc] * id;
                 double p = (d * fc.gm1) * (wl[4 * kWC + cc] * id - 0.5 * (u * u + v * v + w * w));
-                double Tk = p / (kR * d);
-                tau0 = viscosity(fc, Tk) / p;
+                double Tk = p * id * (1.0 / kR);
+                tau0 = collision_time(fc, Tk, p);
             }
             const long long ci = cell0 + (long long)(f + 3) * st.sn;
             // the accumulator of this cell (y, z sweeps) travels to shared memory while the flux
