@@ -67,8 +67,11 @@ struct Phys {
 // Linear weights 1/20, 9/20, 9/20, 1/20; IS_3 replaced by max(IS_0..IS_3);
 // alpha_k = g_k / (eps + IS_k).  The normalised weights are formed with one
 // division: w_k = g_k prod_{m!=k}(eps+IS_m) / sum_m g_m prod_{m'!=m}(eps+IS_m').
-template <class T>
-GKM_HD void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
+// ND: return the double-precision form's numerators and denominators (o0..o3 = Nl, Dl,
+// Nr, Dr, so a caller can share one division among several scalars); else o0, o1 =
+// the reconstructed left and right values.
+template <class T, bool ND>
+GKM_HD void weno_core(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& o0, T& o1, T& o2, T& o3)
 {
     const T c13 = T(1.0 / 3.0), c76 = T(7.0 / 6.0), c116 = T(11.0 / 6.0), c16 = T(1.0 / 6.0), c56 = T(5.0 / 6.0);
     const T c1312 = T(13.0 / 12.0), c14 = T(0.25);
@@ -95,15 +98,16 @@ GKM_HD void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
     I3p = fmax(fmax(fmax(I0p, I1p), I2p), I3p);
     I3n = fmax(fmax(fmax(I0n, I1n), I2n), I3n);
     if constexpr (sizeof(T) == 4) {
+        static_assert(!ND, "the single-precision form has no shared denominators");
         // single precision: products of three (eps + IS) underflow on flat stencils,
         // so form the alphas from reciprocals
         T a0 = T(1) / (eps + I0p), a1 = T(9) / (eps + I1p), a2 = T(9) / (eps + I2p), a3 = T(1) / (eps + I3p);
-        fl = (a0 * P0p + a1 * P1p + a2 * P2p + a3 * P3p) / (a0 + a1 + a2 + a3);
+        o0 = (a0 * P0p + a1 * P1p + a2 * P2p + a3 * P3p) / (a0 + a1 + a2 + a3);
         a0 = T(1) / (eps + I0n);
         a1 = T(9) / (eps + I1n);
         a2 = T(9) / (eps + I2n);
         a3 = T(1) / (eps + I3n);
-        fr = (a0 * P0n + a1 * P1n + a2 * P2n + a3 * P3n) / (a0 + a1 + a2 + a3);
+        o1 = (a0 * P0n + a1 * P1n + a2 * P2n + a3 * P3n) / (a0 + a1 + a2 + a3);
         return;
     }
     T Nl, Dl, Nr, Dr;
@@ -121,16 +125,37 @@ GKM_HD void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
         Nr = n0 * P0n + n1 * P1n + n2 * P2n + n3 * P3n;
         Dr = n0 + n1 + n2 + n3;
     }
+    if constexpr (ND) {
+        o0 = Nl;
+        o1 = Dl;
+        o2 = Nr;
+        o3 = Dr;
+        return;
+    }
 #if GKM_REFERENCE_FORM
-    fl = Nl / Dl;
-    fr = Nr / Dr;
+    o0 = Nl / Dl;
+    o1 = Nr / Dr;
 #else
-    // both sides with one division: D ranges from 4 eps^3 (flat stencil) to (IS_max)^3, so
-    // Dl Dr stays inside the double range for any physical state
+    // both sides with one division: D ranges from 4 eps^3 (flat stencil) to about IS_max^3,
+    // so Dl Dr stays far inside the double range for any physical state
     const T inv = T(1) / (Dl * Dr);
-    fl = Nl * (Dr * inv);
-    fr = Nr * (Dl * inv);
+    o0 = Nl * (Dr * inv);
+    o1 = Nr * (Dl * inv);
 #endif
+}
+
+template <class T>
+GKM_HD void weno_scalar(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& fl, T& fr)
+{
+    T u0, u1;
+    weno_core<T, false>(a3, a2, a1, b1, b2, b3, eps, fl, fr, u0, u1);
+}
+
+// numerators and denominators of both sides (double precision), fl = Nl / Dl, fr = Nr / Dr
+template <class T>
+GKM_HD void weno_nd(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& Nl, T& Dl, T& Nr, T& Dr)
+{
+    weno_core<T, true>(a3, a2, a1, b1, b2, b3, eps, Nl, Dl, Nr, Dr);
 }
 
 // temperature of a conserved state, src/update.cpp:615-620
@@ -154,6 +179,13 @@ GKM_HD T face_energy(T r, T m1, T m2, T m3, T Tf, const Phys<T>& ph)
 #else
     return r * Tf * (ph.Rg / ph.gm1) + T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) / r;
 #endif
+}
+
+// face energy with 1/r given (the sweeps form the two sides' reciprocals together)
+template <class T>
+GKM_HD T face_energy_ir(T r, T ir, T m1, T m2, T m3, T Tf, const Phys<T>& ph)
+{
+    return r * Tf * (ph.Rg / ph.gm1) + T(0.5) * (m1 * m1 + m2 * m2 + m3 * m3) * ir;
 }
 
 // ------------------------------------------------------ moment tables ----

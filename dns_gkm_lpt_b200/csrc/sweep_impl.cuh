@@ -379,18 +379,47 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 const int aa = c / kWB, bb = c - aa * kWB;
                 if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
                 T l[5], r[5];
+                if constexpr (kMixed) {
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const int o = q * kWC + c;
-                    weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], q == 0 ? eps_r : eps_m, l[q], r[q]);
+                    for (int q = 0; q < 4; q++) {
+                        const int o = q * kWC + c;
+                        weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], q == 0 ? eps_r : eps_m, l[q], r[q]);
+                    }
+                    T Tl, Tr;
+                    {
+                        const int o = 5 * kWC + c;
+                        weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], eps_T, Tl, Tr);
+                    }
+                    l[4] = face_energy<T>(l[0], l[1], l[2], l[3], Tl, ph);
+                    r[4] = face_energy<T>(r[0], r[1], r[2], r[3], Tr, ph);
+                } else {
+                    // FP64: the weighted averages of (rho, rho u) and of (rho v, rho w) each share one
+                    // division among their four denominators (each between 4 eps^3 and about IS^3,
+                    // so the product of four stays inside the double range), T takes one, and the
+                    // two face energies share the reciprocal of rho_l rho_r
+                    T N[5][2], D[5][2];
+#pragma unroll
+                    for (int q = 0; q < 5; q++) {
+                        const int o = (q < 4 ? q : 5) * kWC + c;
+                        weno_nd<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], q == 0 ? eps_r : (q < 4 ? eps_m : eps_T),
+                                   N[q][0], D[q][0], N[q][1], D[q][1]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q += 2) {
+                        const T pa = D[q][0] * D[q][1], pb = D[q + 1][0] * D[q + 1][1];
+                        const T inv = T(1) / (pa * pb);
+                        const T ia = pb * inv, ib = pa * inv;   // 1 / pa, 1 / pb
+                        l[q] = N[q][0] * (D[q][1] * ia);
+                        r[q] = N[q][1] * (D[q][0] * ia);
+                        l[q + 1] = N[q + 1][0] * (D[q + 1][1] * ib);
+                        r[q + 1] = N[q + 1][1] * (D[q + 1][0] * ib);
+                    }
+                    const T iT = T(1) / (D[4][0] * D[4][1]);
+                    const T Tl = N[4][0] * (D[4][1] * iT), Tr = N[4][1] * (D[4][0] * iT);
+                    const T ilr = T(1) / (l[0] * r[0]);
+                    l[4] = face_energy_ir<T>(l[0], r[0] * ilr, l[1], l[2], l[3], Tl, ph);
+                    r[4] = face_energy_ir<T>(r[0], l[0] * ilr, r[1], r[2], r[3], Tr, ph);
                 }
-                T Tl, Tr;
-                {
-                    const int o = 5 * kWC + c;
-                    weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], eps_T, Tl, Tr);
-                }
-                l[4] = face_energy<T>(l[0], l[1], l[2], l[3], Tl, ph);
-                r[4] = face_energy<T>(r[0], r[1], r[2], r[3], Tr, ph);
 #pragma unroll
                 for (int q = 0; q < 5; q++) {
                     rec[q * kWC + c] = l[q];
