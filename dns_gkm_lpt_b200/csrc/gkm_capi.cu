@@ -598,7 +598,8 @@ gkm_status gkm_destroy(gkm_handle* h)
     cudaFree(h->lap_nodes);
     cudaFree(h->props);
     for (cudaEvent_t e : h->pipe_ev) cudaEventDestroy(e);
-    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1], h->pipe_comp[2], h->pipe_comp[3]})
+    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1], h->pipe_comp[2], h->pipe_comp[3],
+                           h->pipe_halo})
         if (s) cudaStreamDestroy(s);
     cudaFree(h->partials);
     cudaFree(h->stats_out);
@@ -869,10 +870,10 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     const int S = h->pipe_streams;
     if (!h->pipe_in) {
         for (cudaStream_t* s : {&h->pipe_in, &h->pipe_out, &h->pipe_comp[0], &h->pipe_comp[1], &h->pipe_comp[2],
-                                &h->pipe_comp[3]})
+                                &h->pipe_comp[3], &h->pipe_halo})
             CK(h, cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
     }
-    const size_t nev = 3 * (size_t)K + 2;
+    const size_t nev = 5 * (size_t)K + 2;
     while (h->pipe_ev.size() < nev) {
         cudaEvent_t e;
         CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -882,6 +883,8 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     cudaEvent_t* ev_in = &h->pipe_ev[2];
     cudaEvent_t* ev_out = &h->pipe_ev[2 + K];
     cudaEvent_t* ev_head = &h->pipe_ev[2 + 2 * K];
+    cudaEvent_t* ev_cp_head = &h->pipe_ev[2 + 3 * K];   // copy of chunk c's first planes landed
+    cudaEvent_t* ev_cp_rest = &h->pipe_ev[2 + 4 * K];   // copy of the rest of chunk c landed
     double* Wd = h->buf[h->parity];
     double* A = h->buf[h->parity ^ 1];
     DevClock* ck = h->clock;
@@ -892,7 +895,8 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     CK(h, cudaMemsetAsync(&ck->wave[h->parity ^ 1], 0, sizeof(unsigned long long), h->stream));
     CK(h, cudaMemsetAsync(&ck->status, 0, sizeof(int), h->stream));
     CK(h, cudaEventRecord(ev_start, h->stream));
-    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1], h->pipe_comp[2], h->pipe_comp[3]})
+    for (cudaStream_t s : {h->pipe_in, h->pipe_out, h->pipe_comp[0], h->pipe_comp[1], h->pipe_comp[2], h->pipe_comp[3],
+                           h->pipe_halo})
         CK(h, cudaStreamWaitEvent(s, ev_start, 0));
 
     auto copy_in = [&](int J0, int J1) -> cudaError_t {
@@ -914,28 +918,38 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
         return cudaSuccess;
     };
 
-    // copy-in stream: the last three interior planes first, then per chunk its first three planes
-    // (all that the previous chunk's sweeps need of it) and the rest, each part with its ghosts
+    // copy-in stream, copies only and back to back: the last three interior planes first, then per
+    // chunk its first three planes (all that the previous chunk's sweeps need of it) and the rest.
+    // The halo stream wraps each part's ghosts once it has landed (a kernel between the copies
+    // would leave the copy engine idle while it runs).
     CK(h, copy_in(n, n + 3));
     for (int c = 0; c < K; c++) {
         const int J0 = 3 + B[c], J1 = 3 + B[c + 1];
         const int J1c = (J0 < n) ? std::min(J1, n) : J1;   // planes n..n+2 are already in
         const int Jh = std::min(J0 + 3, J1), Jhc = std::min(Jh, J1c);
         if (Jhc > J0) CK(h, copy_in(J0, Jhc));
-        if (c == 0) {
-            CK(h, gkm::launch_halo_planes(Wd, fc, 0, 3, h->pipe_in));
-            CK(h, gkm::launch_halo_planes(Wd, fc, n + 3, n + 6, h->pipe_in));
+        CK(h, cudaEventRecord(ev_cp_head[c], h->pipe_in));
+        if (J1c > Jhc) CK(h, copy_in(Jhc, J1c));
+        CK(h, cudaEventRecord(ev_cp_rest[c], h->pipe_in));
+    }
+    for (int c = 0; c < K; c++) {
+        const int J0 = 3 + B[c], J1 = 3 + B[c + 1];
+        const int Jh = std::min(J0 + 3, J1);
+        CK(h, cudaStreamWaitEvent(h->pipe_halo, ev_cp_head[c], 0));
+        if (c == 0) {   // the y-ghost planes: images of planes n..n+2 (copied first) and of chunk 0's head
+            CK(h, gkm::launch_halo_planes(Wd, fc, 0, 3, h->pipe_halo));
+            CK(h, gkm::launch_halo_planes(Wd, fc, n + 3, n + 6, h->pipe_halo));
             h->launches += 2;
         }
-        CK(h, gkm::launch_halo_planes(Wd, fc, J0, Jh, h->pipe_in));
+        CK(h, gkm::launch_halo_planes(Wd, fc, J0, Jh, h->pipe_halo));
         h->launches += 1;
-        CK(h, cudaEventRecord(ev_head[c], h->pipe_in));
-        if (J1c > Jhc) CK(h, copy_in(Jhc, J1c));
+        CK(h, cudaEventRecord(ev_head[c], h->pipe_halo));
+        CK(h, cudaStreamWaitEvent(h->pipe_halo, ev_cp_rest[c], 0));
         if (J1 > Jh) {
-            CK(h, gkm::launch_halo_planes(Wd, fc, Jh, J1, h->pipe_in));
+            CK(h, gkm::launch_halo_planes(Wd, fc, Jh, J1, h->pipe_halo));
             h->launches += 1;
         }
-        CK(h, cudaEventRecord(ev_in[c], h->pipe_in));
+        CK(h, cudaEventRecord(ev_in[c], h->pipe_halo));
     }
 
     // compute: chunk c on compute stream c % S, after its own planes and the first three of chunk c+1

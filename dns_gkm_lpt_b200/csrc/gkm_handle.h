@@ -61,6 +61,7 @@ struct gkm_handle {
     // plug-point pipeline (gkm_evolve with pinned or device buffers): copy-in, copy-out and
     // two compute streams, and per-chunk events, created on first use
     cudaStream_t pipe_in = nullptr, pipe_out = nullptr, pipe_comp[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t pipe_halo = nullptr;   // ghost wrap of each part as it lands, off the copy-in stream
     std::vector<cudaEvent_t> pipe_ev;
     int pipe_chunk = 0;      // y-planes per chunk (multiple of 16); 0: about n/8
     // tensor maps of the two state buffers for the FP64 x / y sweeps' slab copies, in device
