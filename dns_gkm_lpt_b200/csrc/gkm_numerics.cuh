@@ -735,6 +735,35 @@ struct Prim {
     T den, ir, U[3], P, lam, inv2lam;
 };
 
+// both face states together: 1/rho_l and 1/rho_r from one division, 1/p_l, 1/p_r and
+// 1/(p_l + p_r) (the collision-time ratio) from another
+template <class T>
+GKM_HD void prim_pair(const T wl[5], const T wr[5], T gm1, Prim<T>& l, Prim<T>& r, T& inv_psum)
+{
+    l.den = wl[0];
+    r.den = wr[0];
+    const T idd = T(1) / (l.den * r.den);
+    l.ir = r.den * idd;
+    r.ir = l.den * idd;
+    Prim<T>* st[2] = {&l, &r};
+    const T* w[2] = {wl, wr};
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        Prim<T>& s = *st[k];
+        s.U[0] = w[k][1] * s.ir;
+        s.U[1] = w[k][2] * s.ir;
+        s.U[2] = w[k][3] * s.ir;
+        s.P = (s.den * gm1) * (w[k][4] * s.ir - T(0.5) * (s.U[0] * s.U[0] + s.U[1] * s.U[1] + s.U[2] * s.U[2]));
+    }
+    const T psum = l.P + r.P, pp = l.P * r.P;
+    const T ipp = T(1) / (pp * psum);
+    inv_psum = pp * ipp;
+    l.lam = T(0.5) * l.den * (r.P * psum * ipp);
+    r.lam = T(0.5) * r.den * (l.P * psum * ipp);
+    l.inv2lam = l.P * l.ir;
+    r.inv2lam = r.P * r.ir;
+}
+
 template <class T>
 GKM_HD Prim<T> prim(const T W[5], T gm1)
 {
@@ -803,6 +832,7 @@ GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, 
     const int K = ph.K;
     const T iK3 = T(1) / T(K + 3);
     Prim<T> stl, str;
+    T inv_psum;
     {
         T wl[5], wr[5];
 #pragma unroll
@@ -810,14 +840,13 @@ GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, 
             wl[q] = in.Wl(q);
             wr[q] = in.Wr(q);
         }
-        stl = prim<T>(wl, ph.gm1);
-        str = prim<T>(wr, ph.gm1);
+        prim_pair<T>(wl, wr, ph.gm1, stl, str, inv_psum);
     }
 
     // collision time with the pressure-jump correction, src/GKMflux.cpp:156-157:
-    // |rho_l/lam_l - rho_r/lam_r| / |rho_l/lam_l + rho_r/lam_r| with rho/lam = 2 p
+    // |rho_l/lam_l - rho_r/lam_r| / |rho_l/lam_l + rho_r/lam_r| with rho/lam = 2 p (p > 0)
     const TimeCoefs<wide_t<T>> tc = time_coefs<wide_t<T>, (sizeof(T) < sizeof(wide_t<T>))>(
-        wide_t<T>(tau0) + wide_t<T>(dt) * wide_t<T>(fabs(stl.P - str.P) / fabs(stl.P + str.P)), wide_t<T>(dt));
+        wide_t<T>(tau0) + wide_t<T>(dt) * wide_t<T>(fabs(stl.P - str.P) * inv_psum), wide_t<T>(dt));
     const T gm1 = T(tc.gm1), gm2 = T(tc.gm2), gm3 = T(tc.gm3), gm4 = T(tc.gm4), gm5 = T(tc.gm5);
     const T p0 = T(tc.p0), p1 = T(tc.p1), p2 = T(tc.p2), p3 = T(tc.p3), p4 = T(tc.p4), p5 = T(tc.p5);
 

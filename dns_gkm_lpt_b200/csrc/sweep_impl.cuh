@@ -393,10 +393,10 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                     l[4] = face_energy<T>(l[0], l[1], l[2], l[3], Tl, ph);
                     r[4] = face_energy<T>(r[0], r[1], r[2], r[3], Tr, ph);
                 } else {
-                    // FP64: the weighted averages of (rho, rho u) and of (rho v, rho w) each share one
-                    // division among their four denominators (each between 4 eps^3 and about IS^3,
-                    // so the product of four stays inside the double range), T takes one, and the
-                    // two face energies share the reciprocal of rho_l rho_r
+                    // FP64: the weighted averages of rho, rho u, rho v, rho w share one division among
+                    // their eight denominators (each between 20 eps^3 and about IS^3, so the
+                    // product stays far inside the double range for physical states); T and the
+                    // two face energies share a second one (denominators of T, rho_l, rho_r)
                     T N[5][2], D[5][2];
 #pragma unroll
                     for (int q = 0; q < 5; q++) {
@@ -404,19 +404,24 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                         weno_nd<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], q == 0 ? eps_r : (q < 4 ? eps_m : eps_T),
                                    N[q][0], D[q][0], N[q][1], D[q][1]);
                     }
+                    {
+                        T pq[4];
 #pragma unroll
-                    for (int q = 0; q < 4; q += 2) {
-                        const T pa = D[q][0] * D[q][1], pb = D[q + 1][0] * D[q + 1][1];
-                        const T inv = T(1) / (pa * pb);
-                        const T ia = pb * inv, ib = pa * inv;   // 1 / pa, 1 / pb
-                        l[q] = N[q][0] * (D[q][1] * ia);
-                        r[q] = N[q][1] * (D[q][0] * ia);
-                        l[q + 1] = N[q + 1][0] * (D[q + 1][1] * ib);
-                        r[q + 1] = N[q + 1][1] * (D[q + 1][0] * ib);
+                        for (int q = 0; q < 4; q++) pq[q] = D[q][0] * D[q][1];
+                        const T p01 = pq[0] * pq[1], p23 = pq[2] * pq[3];
+                        const T inv = T(1) / (p01 * p23);
+                        const T i01 = p23 * inv, i23 = p01 * inv;   // 1 / p01, 1 / p23
+                        const T iq[4] = {pq[1] * i01, pq[0] * i01, pq[3] * i23, pq[2] * i23};
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            l[q] = N[q][0] * (D[q][1] * iq[q]);
+                            r[q] = N[q][1] * (D[q][0] * iq[q]);
+                        }
                     }
-                    const T iT = T(1) / (D[4][0] * D[4][1]);
+                    const T pT = D[4][0] * D[4][1], plr = l[0] * r[0];
+                    const T inv2 = T(1) / (pT * plr);
+                    const T iT = plr * inv2, ilr = pT * inv2;   // 1 / pT, 1 / (rho_l rho_r)
                     const T Tl = N[4][0] * (D[4][1] * iT), Tr = N[4][1] * (D[4][0] * iT);
-                    const T ilr = T(1) / (l[0] * r[0]);
                     l[4] = face_energy_ir<T>(l[0], r[0] * ilr, l[1], l[2], l[3], Tl, ph);
                     r[4] = face_energy_ir<T>(r[0], l[0] * ilr, r[1], r[2], r[3], Tr, ph);
                 }
