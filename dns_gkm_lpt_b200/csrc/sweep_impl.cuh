@@ -90,9 +90,10 @@ __device__ __forceinline__ double collision_time(const FieldConst& fc, double T,
     return fc.mu0 * (x * sqrt(x)) * (fc.T0 + 110.4) / ((T + 110.4) * p);
 }
 
-// |u| + c of a conserved state in FP64: with one reciprocal of rho (the mixed form, whose
-// fields carry FP32 flux errors anyway), and with the reference's divisions
-// (src/update.cpp:1039-1046 via c2p), which give the FP64 form's dt bit for bit.
+// |u| + c of a conserved state in FP64: with one reciprocal of rho (the z sweeps' reduction
+// for the next step's dt, within an ulp or two of the reference's), and with the reference's
+// divisions (src/update.cpp:1039-1046 via c2p; the stand-alone timestep, whose dt equals the
+// reference's bit for bit).
 __device__ __forceinline__ double wave_speed_recip(const double w[5], double gam, double gm1)
 {
     const double d = w[0], id = 1.0 / d;
@@ -273,6 +274,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     const T eps_m = kMixed ? T(fc.eps_m) : T(kWenoEps);
     const T eps_T = kMixed ? T(fc.eps_T) : T(kWenoEps);
     const double* __restrict__ W = a.W;
+    const double suth_c = fc.mu0 * (fc.T0 + 110.4) * kR / ((kR * fc.T0) * sqrt(kR * fc.T0));
 
     if (DIR == 0 && bx == 0 && by == 0 && bz == 0 && tid == 0 && !a.skip_clock_init) {
         a.clock->wave[a.parity ^ 1] = 0ull;   // the z sweep of this step reduces into it
@@ -466,12 +468,17 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 const float p = (d * float(fc.gm1)) * (wl[4 * kWC + cc] * id - 0.5f * (u * u + v * v + w * w));
                 const double Tk = (double)(p * id) * fc.T0;
                 tau0 = T(collision_time(fc, Tk, (double)p * fc.p0) * fc.u_s * fc.inv_dx);
-            } else {
+            } else if (fc.visc == 1) {
                 double d = wl[cc], id = 1.0 / d;
                 double u = wl[kWC + cc] * id, v = wl[2 * kWC + cc] * id, w = wl[3 * kWC + cc] * id;
                 double p = (d * fc.gm1) * (wl[4 * kWC + cc] * id - 0.5 * (u * u + v * v + w * w));
-                double Tk = p * id * (1.0 / kR);
-                tau0 = collision_time(fc, Tk, p);
+                tau0 = collision_time(fc, p * id * (1.0 / kR), p);
+            } else {
+                // Sutherland with pd = p rho = (gamma - 1)(E rho - |m|^2 / 2): T = pd / (R rho^2) and
+                // mu(T) / p = C sqrt(pd) / (pd + 110.4 R rho^2), C = mu0 (T0 + 110.4) R / (R T0)^(3/2)
+                const double d = wl[cc], m1 = wl[kWC + cc], m2 = wl[2 * kWC + cc], m3 = wl[3 * kWC + cc];
+                const double pd = fc.gm1 * (wl[4 * kWC + cc] * d - 0.5 * (m1 * m1 + m2 * m2 + m3 * m3));
+                tau0 = suth_c * sqrt(pd) / (pd + (110.4 * kR) * (d * d));
             }
             const long long ci = cell0 + (long long)(f + 3) * st.sn;
             // the accumulator of this cell (y, z sweeps) travels to shared memory while the flux
@@ -514,7 +521,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                         wn[q] = __dsub_rn(wq, __dmul_rn(fc.inv_dx, s));
                         a.A[q * nt3 + ci] = wn[q];
                     }
-                    const double ws = kMixed ? wave_speed_recip(wn, fc.gam, fc.gm1) : wave_speed(wn, fc.gam, fc.gm1);
+                    const double ws = wave_speed_recip(wn, fc.gam, fc.gm1);
                     if (!isfinite(ws) || !(wn[0] > 0.0)) bad = true;
                     else wmax = ws > wmax ? ws : wmax;
                 }
