@@ -10,9 +10,11 @@ Checks
     fields rel-L2 <= 1e-13, particles <= 1e-12, clocks equal (the per-member
     arithmetic is the single-cube code; the report says whether it was bit
     for bit);
-  * the same for the mixed-precision form (FP32 flux): fields <= 1e-6 and
+  * the same for the mixed-precision form (FP32 flux): fields <= 3e-6 and
     particles <= 1e-6 against the single mixed cube (FP32 rounding differs
-    between the two kernel builds), fields <= 1e-5 against FP64;
+    between the two kernel builds, and each build is about 1e-6 from FP64
+    after these steps, so two builds may differ by twice that), fields <= 1e-5
+    against FP64;
   * graph replay == the event-timed path; autotuning keeps the state;
   * member handles refuse gkm_destroy / gkm_set_stream and a member stepped
     outside the ensemble stops the ensemble with GKM_ERR_STATE.
@@ -131,7 +133,7 @@ def test_ensemble_members_match_single_cubes_fp64():
 def test_ensemble_members_match_single_cubes_mixed():
     single = _single_runs(1, 6)
     ens = _ensemble_runs(1, 6)
-    _compare(ens, single, 1e-6, 1e-6, "mixed ensemble vs single mixed cubes", clock_tol=1e-6)
+    _compare(ens, single, 3e-6, 1e-6, "mixed ensemble vs single mixed cubes", clock_tol=1e-6)
     fp64 = _single_runs(0, 6)
     for m, (x, y) in enumerate(zip(ens, fp64)):
         assert rel_l2(x[0], y[0]).max() <= 1e-5, m
