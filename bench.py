@@ -42,7 +42,7 @@ REF_PART = N_PART * REF_N ** 3 // N_CELLS ** 3   # same particle density
 HBM_PEAK_GBS = 6550.7        # measured copy bandwidth of this pool's B200s
 # DRAM bytes per cell of one sweep launch, from the ncu capture of a 128^3 case (traffic scales with
 # the cells a launch processes; mean over the x, y, z sweeps)
-SWEEP_DRAM_BYTES_PER_CELL = 101.9   # profiles/sweep_kernel_fp64_128cube_full.md, mean of x/y/z
+SWEEP_DRAM_BYTES_PER_CELL = 97.9   # mean DRAM bytes per cell of the x, y, z sweep launches (ncu, 128^3)
 
 
 # batched ensemble: 16 x 32^3 + 8 x 48^3 + 6 x 64^3 + 2 x 96^3 (4.75 M cells), Mt ~ U[0.1, 0.6],
