@@ -37,6 +37,22 @@ void hn_flux_double(const double* in, double gam, double dt, double dx, double* 
     gks_flux<double>(f, in[50], dt, dx, ph, F);
 }
 
+// the same face with the reference's moment algebra (one MCal per table, weight and slope)
+void hn_flux_double_mcal(const double* in, double gam, double dt, double dx, double* F)
+{
+    Face<double> f;
+    for (int q = 0; q < 5; q++) {
+        f.WL_[q] = in[q];
+        f.WR_[q] = in[5 + q];
+        f.Wl_[q] = in[10 + q];
+        f.Wr_[q] = in[15 + q];
+    }
+    for (int v = 0; v < 6; v++)
+        for (int q = 0; q < 5; q++) f.DW_[v][q] = in[20 + 5 * v + q];
+    const Phys<double> ph{gam, gam - 1.0, kR, (int)((5.0 - 3.0 * gam) / (gam - 1.0))};
+    gks_flux_mcal<double>(f, in[50], dt, dx, ph, F);
+}
+
 // the same face on the mixed-precision path: rho / rho0, m / (rho0 us), E / p0,
 // lengths in dx, times in dx / us, us = sqrt(p0 / rho0); result back in dimensional FP64
 void hn_flux_mixed(const double* in, double gam, double dt, double dx, double den0, double p0, double* F)
