@@ -377,7 +377,12 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             const T* s3 = slot(f + 1);
             const T* s4 = slot(f + 2);
             const T* s5 = slot(f + 3);
-            for (int c = tid; c < kWC; c += kSweepThreads) {
+            // FP64: one whole cell per thread, the window's remaining cells split into single WENO
+            // scalars below (the remainder would otherwise take a full second round of a few
+            // warps while the others wait at the barrier: 256^3 sweeps -1.7 %; no gain for FP32)
+            constexpr bool kSplit = !kMixed && kWC > kSweepThreads;
+            const int c_end = kSplit ? kSweepThreads : kWC;
+            for (int c = tid; c < c_end; c += kSweepThreads) {
                 const int aa = c / kWB, bb = c - aa * kWB;
                 if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
                 T l[5], r[5];
@@ -431,6 +436,31 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 for (int q = 0; q < 5; q++) {
                     rec[q * kWC + c] = l[q];
                     rec[(5 + q) * kWC + c] = r[q];
+                }
+            }
+            // the window's cells beyond one per thread: one WENO scalar per work item (5 per cell,
+            // T into the energy slots), then their face energies
+            if constexpr (kSplit) {
+                constexpr int kRest = kWC - kSweepThreads;
+                for (int it = tid; it < 5 * kRest; it += kSweepThreads) {
+                    const int q = it / kRest, c = kSweepThreads + (it - q * kRest);
+                    const int aa = c / kWB, bb = c - aa * kWB;
+                    if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
+                    const int o = (q < 4 ? q : 5) * kWC + c;
+                    T fl, fr;
+                    weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], q == 0 ? eps_r : (q < 4 ? eps_m : eps_T),
+                                   fl, fr);
+                    rec[q * kWC + c] = fl;
+                    rec[(5 + q) * kWC + c] = fr;
+                }
+                __syncthreads();
+                for (int c = kSweepThreads + tid; c < kWC; c += kSweepThreads) {
+                    const int aa = c / kWB, bb = c - aa * kWB;
+                    if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
+                    T* lc = rec + c;
+                    T* rc = rec + 5 * kWC + c;
+                    lc[4 * kWC] = face_energy<T>(lc[0], lc[kWC], lc[2 * kWC], lc[3 * kWC], lc[4 * kWC], ph);
+                    rc[4 * kWC] = face_energy<T>(rc[0], rc[kWC], rc[2 * kWC], rc[3 * kWC], rc[4 * kWC], ph);
                 }
             }
         }
