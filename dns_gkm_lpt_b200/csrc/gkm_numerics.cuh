@@ -75,6 +75,7 @@ GKM_HD void weno_core(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& o0, T& o1, T
 {
     const T c13 = T(1.0 / 3.0), c76 = T(7.0 / 6.0), c116 = T(11.0 / 6.0), c16 = T(1.0 / 6.0), c56 = T(5.0 / 6.0);
     const T c1312 = T(13.0 / 12.0), c14 = T(0.25);
+#if GKM_REFERENCE_FORM
     // candidate polynomials (left-biased "p", right-biased "n")
     T P0p = a3 * c13 - a2 * c76 + a1 * c116;
     T P0n = b3 * c13 - b2 * c76 + b1 * c116;
@@ -95,6 +96,27 @@ GKM_HD void weno_core(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& o0, T& o1, T
     d = b1 - T(2) * a1 + a2; e = -T(3) * b1 + T(4) * a1 - a2; T I2n = c1312 * d * d + c14 * e * e;
     d = b1 - T(2) * b2 + b3; e = -T(5) * b1 + T(8) * b2 - T(3) * b3; T I3p = c1312 * d * d + c14 * e * e;
     d = a1 - T(2) * a2 + a3; e = -T(5) * a1 + T(8) * a2 - T(3) * a3; T I3n = c1312 * d * d + c14 * e * e;
+#else
+    // the left-biased candidate k and the right-biased candidate 3-k are the same polynomial
+    // of the same three cells, and so are the second differences of their indicators: four of
+    // each instead of eight
+    const T Pa = a3 * c13 - a2 * c76 + a1 * c116;   // P0p = P3n
+    const T Pb = -a2 * c16 + a1 * c56 + b1 * c13;   // P1p = P2n
+    const T Pc = a1 * c13 + b1 * c56 - b2 * c16;    // P2p = P1n
+    const T Pd = b1 * c116 - b2 * c76 + b3 * c13;   // P3p = P0n
+    const T P0p = Pa, P3n = Pa, P1p = Pb, P2n = Pb, P2p = Pc, P1n = Pc, P3p = Pd, P0n = Pd;
+    const T dA = a3 - T(2) * a2 + a1, dB = a2 - T(2) * a1 + b1, dC = a1 - T(2) * b1 + b2, dD = b1 - T(2) * b2 + b3;
+    const T qA = c1312 * dA * dA, qB = c1312 * dB * dB, qC = c1312 * dC * dC, qD = c1312 * dD * dD;
+    T e;
+    e = a3 - T(4) * a2 + T(3) * a1;         T I0p = qA + c14 * e * e;
+    e = b3 - T(4) * b2 + T(3) * b1;         T I0n = qD + c14 * e * e;
+    e = b1 - a2;                            T I1p = qB + c14 * e * e;
+    e = a1 - b2;                            T I1n = qC + c14 * e * e;
+    e = -T(3) * a1 + T(4) * b1 - b2;        T I2p = qC + c14 * e * e;
+    e = -T(3) * b1 + T(4) * a1 - a2;        T I2n = qB + c14 * e * e;
+    e = -T(5) * b1 + T(8) * b2 - T(3) * b3; T I3p = qD + c14 * e * e;
+    e = -T(5) * a1 + T(8) * a2 - T(3) * a3; T I3n = qA + c14 * e * e;
+#endif
     I3p = fmax(fmax(fmax(I0p, I1p), I2p), I3p);
     I3n = fmax(fmax(fmax(I0n, I1n), I2n), I3n);
     if constexpr (sizeof(T) == 4) {
