@@ -751,52 +751,60 @@ GKM_HD void contract(T out[5], const T* N, const Tau<T>& t)
 }
 
 // Primitive values of a state with the reciprocals the flux reuses: 1/rho,
-// lam = rho / (2 p) and 1 / (2 lam) = p / rho from one reciprocal of p.
+// lam = rho / (2 p) and 1 / (2 lam) = p / rho.
 template <class T>
 struct Prim {
     T den, ir, U[3], P, lam, inv2lam;
 };
 
-// both face states together: 1/rho_l and 1/rho_r from one division, 1/p_l, 1/p_r and
-// 1/(p_l + p_r) (the collision-time ratio) from another
+// both face states together, with pd = p rho = (gamma - 1)(E rho - |m|^2 / 2) known before any
+// division: 1/rho_l, 1/rho_r, 1/p_l, 1/p_r and 1/(p_l + p_r) (the collision-time ratio) all
+// from one reciprocal of rho_l rho_r pd_l pd_r S, S = pd_l rho_r + pd_r rho_l = (p_l + p_r) rho_l rho_r
 template <class T>
 GKM_HD void prim_pair(const T wl[5], const T wr[5], T gm1, Prim<T>& l, Prim<T>& r, T& inv_psum)
 {
     l.den = wl[0];
     r.den = wr[0];
-    const T idd = T(1) / (l.den * r.den);
-    l.ir = r.den * idd;
-    r.ir = l.den * idd;
+    const T pdl = gm1 * (wl[4] * l.den - T(0.5) * (wl[1] * wl[1] + wl[2] * wl[2] + wl[3] * wl[3]));
+    const T pdr = gm1 * (wr[4] * r.den - T(0.5) * (wr[1] * wr[1] + wr[2] * wr[2] + wr[3] * wr[3]));
+    const T dd = l.den * r.den, pp = pdl * pdr;
+    const T S = pdl * r.den + pdr * l.den;
+    const T inv = T(1) / ((dd * pp) * S);
+    const T ppS = pp * S * inv;   // 1 / dd
+    l.ir = r.den * ppS;
+    r.ir = l.den * ppS;
+    const T ddS = dd * S * inv;   // 1 / pp
+    const T iPl = l.den * (pdr * ddS), iPr = r.den * (pdl * ddS);   // rho / pd
+    inv_psum = dd * (dd * pp * inv);
     Prim<T>* st[2] = {&l, &r};
     const T* w[2] = {wl, wr};
+    const T pd[2] = {pdl, pdr}, iP[2] = {iPl, iPr};
 #pragma unroll
     for (int k = 0; k < 2; k++) {
         Prim<T>& s = *st[k];
         s.U[0] = w[k][1] * s.ir;
         s.U[1] = w[k][2] * s.ir;
         s.U[2] = w[k][3] * s.ir;
-        s.P = (s.den * gm1) * (w[k][4] * s.ir - T(0.5) * (s.U[0] * s.U[0] + s.U[1] * s.U[1] + s.U[2] * s.U[2]));
+        s.P = pd[k] * s.ir;
+        s.lam = T(0.5) * s.den * iP[k];
+        s.inv2lam = s.P * s.ir;
     }
-    const T psum = l.P + r.P, pp = l.P * r.P;
-    const T ipp = T(1) / (pp * psum);
-    inv_psum = pp * ipp;
-    l.lam = T(0.5) * l.den * (r.P * psum * ipp);
-    r.lam = T(0.5) * r.den * (l.P * psum * ipp);
-    l.inv2lam = l.P * l.ir;
-    r.inv2lam = r.P * r.ir;
 }
 
+// one state with one division: 1/rho = pd / (rho pd), 1/p = rho^2 / (rho pd)
 template <class T>
 GKM_HD Prim<T> prim(const T W[5], T gm1)
 {
     Prim<T> s;
     s.den = W[0];
-    s.ir = T(1) / s.den;
+    const T pd = gm1 * (W[4] * s.den - T(0.5) * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]));
+    const T inv = T(1) / (s.den * pd);
+    s.ir = pd * inv;
     s.U[0] = W[1] * s.ir;
     s.U[1] = W[2] * s.ir;
     s.U[2] = W[3] * s.ir;
-    s.P = (s.den * gm1) * (W[4] * s.ir - T(0.5) * (s.U[0] * s.U[0] + s.U[1] * s.U[1] + s.U[2] * s.U[2]));
-    s.lam = T(0.5) * s.den * (T(1) / s.P);
+    s.P = pd * s.ir;
+    s.lam = T(0.5) * s.den * (s.den * s.den * inv);
     s.inv2lam = s.P * s.ir;
     return s;
 }
