@@ -30,6 +30,10 @@ __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, 
 // component-batched launches (fewer lines per component, more inputs in flight pay), U = 4 for
 // the one-component launches of large grids (their lines already fill the GPU).
 constexpr int kLineBatchBatched = 8, kLineBatchSingle = 4;
+// the component-batched pass kernels hold six 128-thread CTAs per SM (80 registers): more lines
+// in flight than the compiler's own choice (96-112 registers; 256^3 splines 1.57 -> 1.49 ms),
+// where eight (64 registers) spill the fetch-ahead values
+constexpr int kPassCtasPerSm = 6;
 
 template <int U, class Src>
 __device__ void line_solve(const Src& f, int N, int periodic, const SplineTables& tb, double* c, long long cs)
@@ -866,7 +870,7 @@ cudaError_t grid_launch(K kernel, long long work, int threads, cudaStream_t s, A
 }
 
 // ---- ensemble forms: one launch per pass over every member's lines / particles
-__global__ void ensemble_pass0_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm,
+__global__ void __launch_bounds__(128, kPassCtasPerSm) ensemble_pass0_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm,
                                       int buf)
 {
     const long long total = off[nm];
@@ -880,7 +884,7 @@ __global__ void ensemble_pass0_kernel(const MemberDev* __restrict__ mem, const l
     }
 }
 
-__global__ void ensemble_pass1_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm)
+__global__ void __launch_bounds__(128, kPassCtasPerSm) ensemble_pass1_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm)
 {
     const long long total = off[nm];
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
@@ -893,7 +897,7 @@ __global__ void ensemble_pass1_kernel(const MemberDev* __restrict__ mem, const l
     }
 }
 
-__global__ void __launch_bounds__(32 * kPass2Warps)
+__global__ void __launch_bounds__(32 * kPass2Warps, kPassCtasPerSm)
     ensemble_pass2_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm)
 {
     __shared__ double stage[kPass2Warps][32][kLineChunk + 1];
