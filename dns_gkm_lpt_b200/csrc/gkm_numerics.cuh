@@ -9,12 +9,13 @@
 //   slope solve       src/GKMflux.cpp:283-297
 //   c2p               src/GKMflux.cpp:302-309
 //
-// The flux is reorganised for registers, not re-derived: every moment product
-// of the reference is formed, but each slope vector is consumed as soon as it
-// is known (its contributions to the tangential/A-slope right-hand sides and
-// to the flux are accumulated at once), so only one side's moment tables are
-// live at a time.  Divisions by per-face constants become multiplications by
-// one reciprocal.  The results differ from the reference only by rounding.
+// Two forms of the flux.  gks_flux_mcal keeps the reference's moment algebra
+// (one MCal per table, weight and slope vector) and is what the operation
+// counter measures.  gks_flux_tau, the one the kernels run, takes the same
+// moments of the same slope vectors as contractions of the normal tables with
+// tangential functionals of each slope polynomial, and forms each reciprocal
+// once (grouped divisions, one reciprocal square root per state).  The two
+// forms and the reference differ only by rounding.
 #pragma once
 
 #include <math.h>
@@ -41,10 +42,6 @@
 // side code per side) or one loop body.
 #ifndef GKM_UNROLL_SIDES
 #define GKM_UNROLL_SIDES 1
-#endif
-// Dot products of the moment contractions summed pairwise (shorter dependency chains).
-#ifndef GKM_TREE_SUMS
-#define GKM_TREE_SUMS 0
 #endif
 
 namespace gkm {
@@ -350,17 +347,10 @@ GKM_HD void mcal(T M[5], const T* I, GKM_YZ_PARAM, T Ie2, T Ie4, const T a[5])
     T v1 = T(0.5) * (TM(3, 0, 0) + TM(1, 2, 0) + TM(1, 0, 2) + t100 * Ie2);
     T v2 = T(0.5) * (TM(2, 1, 0) + TM(0, 3, 0) + TM(0, 1, 2) + t010 * Ie2);
     T v3 = T(0.5) * (TM(2, 0, 1) + TM(0, 2, 1) + TM(0, 0, 3) + t001 * Ie2);
-#if GKM_TREE_SUMS
-    M[0] = (a[0] * t000 + a[1] * t100) + (a[2] * t010 + a[3] * t001) + a[4] * v0;
-    M[1] = (a[0] * t100 + a[1] * t200) + (a[2] * t110 + a[3] * t101) + a[4] * v1;
-    M[2] = (a[0] * t010 + a[1] * t110) + (a[2] * t020 + a[3] * t011) + a[4] * v2;
-    M[3] = (a[0] * t001 + a[1] * t101) + (a[2] * t011 + a[3] * t002) + a[4] * v3;
-#else
     M[0] = a[0] * t000 + a[1] * t100 + a[2] * t010 + a[3] * t001 + a[4] * v0;
     M[1] = a[0] * t100 + a[1] * t200 + a[2] * t110 + a[3] * t101 + a[4] * v1;
     M[2] = a[0] * t010 + a[1] * t110 + a[2] * t020 + a[3] * t011 + a[4] * v2;
     M[3] = a[0] * t001 + a[1] * t101 + a[2] * t011 + a[3] * t002 + a[4] * v3;
-#endif
     M[4] = T(0.25) * a[4] *
                (TM(4, 0, 0) + TM(0, 4, 0) + TM(0, 0, 4) + t000 * Ie4 +
                 T(2) * (TM(2, 2, 0) + TM(2, 0, 2) + t200 * Ie2 + TM(0, 2, 2) + t020 * Ie2 + t002 * Ie2)) +
