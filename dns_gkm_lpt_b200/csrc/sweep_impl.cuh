@@ -147,9 +147,19 @@ __host__ __device__ constexpr size_t sweep_ring_bytes()
 
 // ring + reconstructions, then a per-thread FP64 staging area [5][threads] for the
 // accumulator of the thread's cell, fetched asynchronously while the flux is computed
-template <class T, class Tile>
+// the mixed x and z sweeps use neither the staging area nor the aligned ring (no tensor copies):
+// their ring and reconstructions alone (3 CTAs: 97.6 KB instead of 115 KB per SM, so more of the
+// SM's memory stays L1 for the z sweep's strided loads; 256^3 mixed sweeps -1.8 %)
+template <class T, int DIR>
+__host__ __device__ constexpr bool sweep_lean()
+{
+    return sizeof(T) == 4 && DIR != 1;
+}
+
+template <class T, class Tile, int DIR = 1>
 __host__ __device__ constexpr size_t sweep_smem_bytes()
 {
+    if (sweep_lean<T, DIR>()) return sizeof(T) * (size_t)(kRing * slot_elems<T, Tile>() + 10 * Tile::WC);
     return sweep_ring_bytes<T, Tile>() + sizeof(double) * 5 * (size_t)Tile::threads + 16;   // + mbarrier
 }
 
@@ -252,7 +262,8 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     constexpr int kSlot = slot_elems<T, Tile>();
     // ring [kRing][kSlot] (slot: kSlabComps x kWC values), reconstructions [10][kWC], then the
     // accumulator staging [5][threads] and one mbarrier
-    T* ring = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    T* ring = sweep_lean<T, DIR>() ? reinterpret_cast<T*>(smem_raw)
+                                   : reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     T* rec = ring + kRing * kSlot;
     double* stage = reinterpret_cast<double*>(smem_raw + sweep_ring_bytes<T, Tile>());   // [5][threads]
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(stage + 5 * kSweepThreads);
@@ -625,7 +636,8 @@ cudaError_t launch_sweep_rows_t(int dir, SweepArgs a, int j0, int j1, cudaStream
     const int n = a.fc.n;
     if (j0 < 0 || j1 > n || j0 >= j1) return cudaErrorInvalidValue;
     const int gb = (n + Tile::TB - 1) / Tile::TB;
-    const size_t smem = sweep_detail::sweep_smem_bytes<T, Tile>();
+    const size_t smem = sweep_detail::sweep_smem_bytes<T, Tile, 1>();
+    const size_t smem0 = sweep_detail::sweep_smem_bytes<T, Tile, 0>(), smem2 = sweep_detail::sweep_smem_bytes<T, Tile, 2>();
     const dim3 block(Tile::TB, Tile::TA);
     if (dir == 1) {
         if (a.seg_len < 1) return cudaErrorInvalidValue;
@@ -638,8 +650,8 @@ cudaError_t launch_sweep_rows_t(int dir, SweepArgs a, int j0, int j1, cudaStream
     if (j0 % Tile::TA) return cudaErrorInvalidValue;
     a.tile_a0 = j0 / Tile::TA;
     const dim3 grid(gb, (j1 + Tile::TA - 1) / Tile::TA - a.tile_a0, (n + a.seg_len - 1) / a.seg_len);
-    if (dir == 0) sweep_kernel<0, T, Tile><<<grid, block, smem, s>>>(a);
-    else sweep_kernel<2, T, Tile><<<grid, block, smem, s>>>(a);
+    if (dir == 0) sweep_kernel<0, T, Tile><<<grid, block, smem0, s>>>(a);
+    else sweep_kernel<2, T, Tile><<<grid, block, smem2, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -647,12 +659,17 @@ template <class T, class Tile>
 cudaError_t launch_ensemble_sweep_t(int dir, const MemberDev* mem, const long long* off, int nm, int parity,
                                     int seg_len, cudaStream_t s)
 {
-    const size_t smem = sweep_detail::sweep_smem_bytes<T, Tile>();
     const dim3 block(Tile::TB, Tile::TA);
     const int grid = 148 * Tile::ctas;
-    if (dir == 0) ensemble_sweep_kernel<0, T, Tile><<<grid, block, smem, s>>>(mem, off, nm, parity, seg_len);
-    else if (dir == 1) ensemble_sweep_kernel<1, T, Tile><<<grid, block, smem, s>>>(mem, off, nm, parity, seg_len);
-    else ensemble_sweep_kernel<2, T, Tile><<<grid, block, smem, s>>>(mem, off, nm, parity, seg_len);
+    if (dir == 0)
+        ensemble_sweep_kernel<0, T, Tile>
+            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 0>(), s>>>(mem, off, nm, parity, seg_len);
+    else if (dir == 1)
+        ensemble_sweep_kernel<1, T, Tile>
+            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 1>(), s>>>(mem, off, nm, parity, seg_len);
+    else
+        ensemble_sweep_kernel<2, T, Tile>
+            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 2>(), s>>>(mem, off, nm, parity, seg_len);
     return cudaGetLastError();
 }
 

@@ -20,7 +20,7 @@ cudaError_t launch_one_mixed(const SweepArgs& a, int nseg, cudaStream_t s)
     using Tile = SweepTile32a;
     dim3 grid((a.fc.n + Tile::TB - 1) / Tile::TB, (a.fc.n + Tile::TA - 1) / Tile::TA, nseg);
     dim3 block(Tile::TB, Tile::TA);
-    sweep_kernel<DIR, float, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<float, Tile>(), s>>>(a);
+    sweep_kernel<DIR, float, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<float, Tile, DIR>(), s>>>(a);
     return cudaGetLastError();
 }
 
