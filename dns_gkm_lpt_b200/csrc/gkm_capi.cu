@@ -834,11 +834,12 @@ bool async_capable(const double* p)
 
 // The plug point evolve(W, dt) as a pipeline over chunks of y-planes: the host -> device copy of
 // chunk c+1, the x/y/z sweeps of chunk c and the device -> host copy of chunk c-1 overlap.  A
-// chunk's sweeps need the input planes within 3 of it (y stencil) with their ghosts; the
-// copy-in stream wraps each chunk's ghosts as it arrives (the periodic y-ghost planes come from
-// the last three interior planes, copied first, and from the first chunk), so chunk c waits for
-// the copy-in of chunk c+1.  Each chunk writes only its own planes of the accumulator, so two
-// compute streams run consecutive chunks concurrently.  Results equal the one-shot path.
+// chunk's sweeps need the input planes within 3 of it (y stencil) with their ghosts; the input
+// arrives in parts that end three planes into the next chunk, and a halo stream wraps each part's
+// ghosts as it lands (the periodic y-ghost planes come from the last three interior planes,
+// copied first, and from the first part), so chunk c waits for part c.  Each chunk writes only
+// its own planes of the accumulator, so two compute streams run consecutive chunks concurrently.
+// Results equal the one-shot path.
 //
 // Chunk boundaries (interior y-planes): the first and the last chunk hold 16 planes, so the
 // sweeps start after a short copy and the copy after the last sweep is short; the others hold C
@@ -873,7 +874,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
                                 &h->pipe_comp[3], &h->pipe_halo})
             CK(h, cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
     }
-    const size_t nev = 5 * (size_t)K + 2;
+    const size_t nev = 3 * (size_t)K + 2;
     while (h->pipe_ev.size() < nev) {
         cudaEvent_t e;
         CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -882,9 +883,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     cudaEvent_t ev_start = h->pipe_ev[0], ev_done_out = h->pipe_ev[1];
     cudaEvent_t* ev_in = &h->pipe_ev[2];
     cudaEvent_t* ev_out = &h->pipe_ev[2 + K];
-    cudaEvent_t* ev_head = &h->pipe_ev[2 + 2 * K];
-    cudaEvent_t* ev_cp_head = &h->pipe_ev[2 + 3 * K];   // copy of chunk c's first planes landed
-    cudaEvent_t* ev_cp_rest = &h->pipe_ev[2 + 4 * K];   // copy of the rest of chunk c landed
+    cudaEvent_t* ev_cp = &h->pipe_ev[2 + 2 * K];   // copy of part c landed
     double* Wd = h->buf[h->parity];
     double* A = h->buf[h->parity ^ 1];
     DevClock* ck = h->clock;
@@ -918,35 +917,31 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
         return cudaSuccess;
     };
 
-    // copy-in stream, copies only and back to back: the last three interior planes first, then per
-    // chunk its first three planes (all that the previous chunk's sweeps need of it) and the rest.
-    // The halo stream wraps each part's ghosts once it has landed (a kernel between the copies
-    // would leave the copy engine idle while it runs).
+    // copy-in stream, copies only and back to back: the last three interior planes first, then one
+    // part per chunk, planes [3 + B[c] + 3, 3 + B[c+1] + 3) (the first part from plane 3, the last
+    // to n + 3): chunk c's planes after its first three, which came with part c-1, and the first
+    // three planes of chunk c+1, all the y stencil of chunk c reaches beyond it.  One copy per
+    // component and part: many small copies in both directions at once lose bus bandwidth.  The
+    // halo stream wraps each part's ghosts once it has landed (a kernel between the copies would
+    // leave the copy engine idle while it runs), and chunk c's sweeps wait for part c.
+    auto part_end = [&](int c) { return c + 1 < K ? std::min(3 + B[c + 1] + 3, n + 3) : n + 3; };
     CK(h, copy_in(n, n + 3));
     for (int c = 0; c < K; c++) {
-        const int J0 = 3 + B[c], J1 = 3 + B[c + 1];
-        const int J1c = (J0 < n) ? std::min(J1, n) : J1;   // planes n..n+2 are already in
-        const int Jh = std::min(J0 + 3, J1), Jhc = std::min(Jh, J1c);
-        if (Jhc > J0) CK(h, copy_in(J0, Jhc));
-        CK(h, cudaEventRecord(ev_cp_head[c], h->pipe_in));
-        if (J1c > Jhc) CK(h, copy_in(Jhc, J1c));
-        CK(h, cudaEventRecord(ev_cp_rest[c], h->pipe_in));
+        const int P0 = c == 0 ? 3 : part_end(c - 1), P1 = part_end(c);
+        const int P1c = std::min(P1, n);   // planes n..n+2 are already in
+        if (P1c > P0) CK(h, copy_in(P0, P1c));
+        CK(h, cudaEventRecord(ev_cp[c], h->pipe_in));
     }
     for (int c = 0; c < K; c++) {
-        const int J0 = 3 + B[c], J1 = 3 + B[c + 1];
-        const int Jh = std::min(J0 + 3, J1);
-        CK(h, cudaStreamWaitEvent(h->pipe_halo, ev_cp_head[c], 0));
-        if (c == 0) {   // the y-ghost planes: images of planes n..n+2 (copied first) and of chunk 0's head
+        const int P0 = c == 0 ? 3 : part_end(c - 1), P1 = part_end(c);
+        CK(h, cudaStreamWaitEvent(h->pipe_halo, ev_cp[c], 0));
+        if (c == 0) {   // the y-ghost planes: images of planes n..n+2 (copied first) and of planes 3..5
             CK(h, gkm::launch_halo_planes(Wd, fc, 0, 3, h->pipe_halo));
             CK(h, gkm::launch_halo_planes(Wd, fc, n + 3, n + 6, h->pipe_halo));
             h->launches += 2;
         }
-        CK(h, gkm::launch_halo_planes(Wd, fc, J0, Jh, h->pipe_halo));
-        h->launches += 1;
-        CK(h, cudaEventRecord(ev_head[c], h->pipe_halo));
-        CK(h, cudaStreamWaitEvent(h->pipe_halo, ev_cp_rest[c], 0));
-        if (J1 > Jh) {
-            CK(h, gkm::launch_halo_planes(Wd, fc, Jh, J1, h->pipe_halo));
+        if (P1 > P0) {
+            CK(h, gkm::launch_halo_planes(Wd, fc, P0, P1, h->pipe_halo));
             h->launches += 1;
         }
         CK(h, cudaEventRecord(ev_in[c], h->pipe_halo));
@@ -964,7 +959,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
     a.skip_clock_init = 1;
     for (int c = 0; c < K; c++) {
         cudaStream_t s = h->pipe_comp[c % S];
-        CK(h, cudaStreamWaitEvent(s, c + 1 < K ? ev_head[c + 1] : ev_in[c], 0));
+        CK(h, cudaStreamWaitEvent(s, ev_in[c], 0));
         const int j0 = B[c], j1 = B[c + 1];
         for (int d = 0; d < 3; d++) {
             gkm::SweepArgs ad = a;
