@@ -15,9 +15,18 @@ N > 1 (torchrun): each rank advances its own independent replica (the path
 does not shard: no inter-GPU exchange); value sums all ranks over the slowest
 rank's time.
 
+"forms" (one GPU): the mixed-precision form on the same 256^3 input; the
+batched ensemble (32 cubes of uneven sizes) in FP64 and mixed precision;
+c2_256_curves, both forms over 200 steps of the 256^3 case with the
+PrintStats curves every 10 steps; c3_512, the 512^3 case (Mt 0.5,
+Re_lambda 100, 4 x 10^6 particles) over 500 steps in both forms, with the
+mixed form's field and curve errors against the FP64 run.
+
 --impl reference: the reference's own CPU code (oracle/_ref, compiled from
-the reference sources) on the host cores, one 64^3 cube per process, all
-processes concurrent, each timed step one reference step.
+the reference sources) on all host cores, one 64^3 cube per process (the
+per-cell rate stands in for the 256^3 cube: extrapolated), all processes
+concurrent, --warmup untimed and --steps timed reference steps each.  The
+GPU arm's cpu_baseline is the same measurement.
 """
 from __future__ import annotations
 
@@ -39,10 +48,25 @@ N_PART = 1_000_000
 MT, RE, CFL, SEED = 0.3, 60.0, 0.5, 1234
 REF_N = 64                   # reference CPU sample: one 64^3 cube per process
 REF_PART = N_PART * REF_N ** 3 // N_CELLS ** 3   # same particle density
-HBM_PEAK_GBS = 6550.7        # measured copy bandwidth of this pool's B200s
+C3_PART = 4_000_000          # particles of the 512^3 mixed-precision case
+HBM_FALLBACK_GBS = 6650.0    # an earlier copy-bandwidth measurement on these B200s, used only without a
+                             # measured-peaks file beside this script
 # DRAM bytes per cell of one sweep launch, from the ncu capture of a 128^3 case (traffic scales with
 # the cells a launch processes; mean over the x, y, z sweeps)
 SWEEP_DRAM_BYTES_PER_CELL = 97.9   # mean DRAM bytes per cell of the x, y, z sweep launches (ncu, 128^3)
+
+
+def hbm_peak():
+    """(GB/s, source) of the HBM copy bandwidth measured on this machine's GPUs (MEASURED_PEAKS.json
+    beside this script, written by the machine's set-up), else the fallback figure."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        if v > 0:
+            return v, "measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
+    return HBM_FALLBACK_GBS, "fallback: earlier copy-bandwidth measurement (no MEASURED_PEAKS.json)"
 
 
 # batched ensemble: 16 x 32^3 + 8 x 48^3 + 6 x 64^3 + 2 x 96^3 (4.75 M cells), Mt ~ U[0.1, 0.6],
@@ -89,7 +113,8 @@ def case_of(n: int):
 
 def workload(n=N_CELLS, npart=N_PART, precision="fp64"):
     Mt, Re = case_of(n)
-    form = "FP64 drop-in" if precision == "fp64" else "mixed precision (FP32 WENO + flux, FP64 state)"
+    form = {"fp64": "FP64 drop-in", "mixed": "mixed precision (FP32 WENO + flux, FP64 state)"}.get(
+        precision, "FP64 drop-in and mixed precision from the same field")
     nt = n + 6
     return {"workload": f"{n}^3 periodic cube, {form}, Mt {Mt}, Re_lambda {Re:g}, {npart} particles, "
                         f"cfl {CFL}, natural_ghost3 splines",
@@ -172,23 +197,34 @@ def run_reference(workers: int, warm: int, steps: int, n=REF_N, npart=REF_PART):
     return {"gcell": gcell, "psteps": psteps, "ms_per_step": ms_step, "workers": workers, "wall_s": wall}
 
 
+def reference_sample_text(workers, warm, steps, wall_s):
+    return (f"{REF_N}^3 cube per process (same spectrum recipe, Mt {MT}, Re_lambda {RE:g}), {REF_PART} particles "
+            f"per process (the 256^3 case's particle density), {workers} concurrent single-rank processes on "
+            f"{workers} host cores, {warm} warm-up + {steps} timed reference steps each ({wall_s:.1f} s wall); "
+            f"Gcell-updates/s is the per-cell rate of those cubes, standing in for the 256^3 cube "
+            f"(extrapolated: a 256^3 step takes ~2 min on one core, and the reference parallelises only "
+            f"through MPI, which this box lacks)")
+
+
+def reference_config(workers):
+    cfg = workload()
+    cfg["workload"] = (f"{cfg['workload']}; reference CPU build measured on {REF_N}^3 cubes, one per process, "
+                       f"x {workers} processes (per-cell rate; stands in for 256^3, extrapolated)")
+    cfg["reference_sample"] = {"n": REF_N, "processes": workers, "particles_per_process": REF_PART}
+    return cfg
+
+
 def reference_arm(args, world: int):
-    ncpu = os.cpu_count() or 1
-    workers = max(1, min(ncpu, 96))
-    # a bounded sample: a reference step of a 64^3 cube takes ~2 s on one core, so at most 10 timed
-    # and 1 warm-up step per process keep the arm within a minute whatever --steps says
-    ref_steps, ref_warm = max(1, min(args.steps, 10)), min(args.warmup, 1)
-    r = run_reference(workers, ref_warm, ref_steps)
-    sample = (f"{REF_N}^3 cube per process (same spectrum recipe, Mt {MT}, Re_lambda {RE:g}), {REF_PART} particles "
-              f"per process, {workers} concurrent processes, {ref_steps} timed reference steps each "
-              f"after {ref_warm} warm-up ({r['wall_s']:.1f} s wall)")
+    workers = max(1, min(os.cpu_count() or 1, 96))
+    # every timed step is one reference step of every process (a 64^3 step takes ~2 s on one core)
+    r = run_reference(workers, args.warmup, args.steps)
     line = {"impl": "reference", "metric": "Gcell-updates/s", "value": r["gcell"], "unit": "Gcell-updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded solenoidal field (init_DNS recipe), uniform particles",
-            "config": workload(), "particle_steps_per_s": r["psteps"],
+            "config": reference_config(workers), "particle_steps_per_s": r["psteps"],
             "cpu_baseline": {"value": r["gcell"], "unit": "Gcell-updates/s", "cores": workers, "kind": "reference",
-                             "sample": sample},
+                             "sample": reference_sample_text(workers, args.warmup, args.steps, r["wall_s"])},
             "e2e": {"value": r["gcell"], "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -295,6 +331,100 @@ def batched_forms(args, local_rank: int, stream):
     return out
 
 
+# ------------------------------------------------ long runs: FP64 vs mixed --
+STAT_KEYS = ("TKE", "Diss", "SijSij", "SKEWu", "SKEWv", "SKEWw", "KURTu", "KURTv", "KURTw", "Prms", "Trms", "Vrms")
+
+
+def long_run_pair(n, npart, steps, seed, local_rank, stream, autotune_reps=2, stats_every=10):
+    """The FP64 drop-in and the mixed-precision form advanced from the same seeded field for
+    `steps` full steps, with the PrintStats line every `stats_every` steps (as the reference prints it,
+    src/update.cpp:135-144, 835-841): per form Gcell-updates/s and particle-steps/s over all steps
+    (CUDA events per phase), and the mixed form's errors against the FP64 run: relative L2 of rho,
+    rho u, rho v, rho w, rho E and of the velocities u, v, w after the last step, and the largest
+    relative difference of every PrintStats curve over the run."""
+    import numpy as np
+    import torch
+
+    from dns_gkm_lpt_b200 import ic
+    from dns_gkm_lpt_b200.solver import Solver
+
+    Mt, Re = case_of(n)
+    dev = f"cuda:{local_rank}"
+    if n > 256:
+        P, W0 = ic.make_state_device(n, Mt, Re, seed, device=dev)
+    else:
+        P, u, v, w, rho, p = ic.make_field(n, Mt, Re, seed)
+        W0 = ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, p))
+        del u, v, w, rho, p
+    pos0 = ic.particles_to_reference_order(ic.make_particles(npart, seed))
+    nt = n + 6
+    out, finals, curves, pos = {}, {}, {}, {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        s = Solver(P, cfl=CFL, max_particles=npart, device=local_rank, precision=prec)
+        s.set_stream(stream.cuda_stream)
+        s.upload_state(W0)
+        s.particles_upload(pos0)
+        cfg = s.autotune(autotune_reps) if autotune_reps > 0 else s.sweep_config()
+        curve, ph_sum, done = [], {}, 0
+        while done < steps:
+            st = s.print_stats()
+            curve.append([st["t_over_t0"]] + [st[k] for k in STAT_KEYS])
+            k = min(stats_every, steps - done)
+            for key, v in s.step_timed(k, True).items():
+                ph_sum[key] = ph_sum.get(key, 0.0) + v
+            done += k
+        st = s.print_stats()
+        curve.append([st["t_over_t0"]] + [st[k] for k in STAT_KEYS])
+        Wf = torch.empty((5, nt, nt, nt), dtype=torch.float64, device=dev)
+        s.download_state(Wf)
+        pos[name] = s.particles_download()[0]
+        s.close()
+        finals[name] = Wf
+        curves[name] = np.array(curve)
+        eul = ph_sum["sweep_x"] + ph_sum["sweep_y"] + ph_sum["sweep_z"] + ph_sum["halo"]
+        part = ph_sum["splines"] + ph_sum["particles"]
+        out[name] = {"value": n ** 3 * steps / (eul * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+                     "particle_steps_per_s": npart * steps / (part * 1e-3),
+                     "ms_per_step": ph_sum["total"] / steps,
+                     "phases_ms_per_step": {k: v / steps for k, v in ph_sum.items()}, "sweep_shapes": cfg}
+    del W0
+    a, b = finals["mixed"], finals["fp64"]
+    sl = (slice(3, nt - 3),) * 3
+
+    def rl2(x, y):
+        return float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
+
+    err = {nm: rl2(a[q][sl], b[q][sl]) for q, nm in enumerate(("rho", "rho_u", "rho_v", "rho_w", "rho_E"))}
+    for q, nm in ((1, "u"), (2, "v"), (3, "w")):
+        err[nm] = rl2(a[q][sl] / a[0][sl], b[q][sl] / b[0][sl])
+    del a, b, finals
+    torch.cuda.empty_cache()
+    cm, cf = curves["mixed"], curves["fp64"]
+    curve_err = {k: float(np.max(np.abs(cm[:, i + 1] - cf[:, i + 1]) / np.maximum(np.abs(cf[:, i + 1]), 1e-300)))
+                 for i, k in enumerate(STAT_KEYS)}
+    # kinetic-energy decay: TKE(t) / TKE(0) of each run
+    decay_m, decay_f = cm[:, 1] / cm[0, 1], cf[:, 1] / cf[0, 1]
+    decay_err = float(np.max(np.abs(decay_m - decay_f) / decay_f))
+    dx = 2 * np.pi / n
+    fields_max = max(err[k] for k in ("rho", "u", "v", "w", "rho_E"))
+    out.update({
+        "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+        "steps": steps, "stats_every": stats_every, "curve_points": len(cf),
+        "rel_l2_mixed_vs_fp64": err,
+        "curve_max_rel_err_mixed_vs_fp64": curve_err,
+        "tke_decay_max_rel_err": decay_err,
+        "t_over_t0_final": {"fp64": float(cf[-1, 0]), "mixed": float(cm[-1, 0])},
+        "tke_decay_final": {"fp64": float(decay_f[-1]), "mixed": float(decay_m[-1])},
+        "particle_pos_max_abs_err": float(np.abs(pos["mixed"] - pos["fp64"]).max()),
+        "particle_cells_equal_fraction": float(np.mean(np.all(
+            np.floor(pos["mixed"] / dx) == np.floor(pos["fp64"] / dx), axis=1))),
+        "bars": {"fields_rel_l2": 1e-5, "tke_decay": 1e-3},
+        "within_bars": bool(fields_max < 1e-5 and decay_err < 1e-3),
+        "curves": {"columns": ["t_over_t0"] + list(STAT_KEYS),
+                   "fp64": cf.tolist(), "mixed": cm.tolist()}})
+    return out
+
+
 # ------------------------------------------------------------- our arm ----
 def ours(args, rank: int, world: int, local_rank: int):
     import numpy as np
@@ -350,7 +480,8 @@ def ours(args, rank: int, world: int, local_rank: int):
     eul_ms, part_ms, total_ms = max_over_ranks([eul_ms, part_ms, total_ms])
     nt = s.nt
     state_bytes = 5 * nt ** 3 * 8
-    do_forms = not args.no_forms and prec == 0
+    # the side forms run on one GPU only (the scaling runs time the main line alone)
+    do_forms = not args.no_forms and prec == 0 and world == 1
     # the particle statistics build five more splines (the 41-column property path): at 1024^3 they
     # do not fit beside the state, the velocity splines and the initial field
     with_pstats = n <= 512
@@ -429,6 +560,22 @@ def ours(args, rank: int, world: int, local_rank: int):
         del W64, Wm
         if not args.no_batched:
             forms.update(batched_forms(args, local_rank, stream))
+        if args.c2_steps > 0:
+            # the 256^3 case over its full run: PrintStats curves of both forms every 10 steps
+            forms["c2_256_curves"] = dict(long_run_pair(256, N_PART, args.c2_steps, SEED, local_rank, stream,
+                                                        args.autotune_reps),
+                                          config=workload(256, N_PART))
+        if args.c3_steps > 0:
+            # the mixed-precision target case: 512^3, Mt 0.5, Re_lambda 100, 4 x 10^6 particles
+            forms["c3_512"] = dict(long_run_pair(512, C3_PART, args.c3_steps, SEED + 512, local_rank, stream,
+                                                 args.autotune_reps),
+                                   config=workload(512, C3_PART, "both"))
+        fp64_256 = world * n ** 3 * args.steps / (eul_ms * 1e-3) / 1e9
+        for key in ("batched_fp64", "batched_mixed"):
+            if key in forms:
+                forms[key]["over_fp64_single_cube_256"] = forms[key]["value"] / fp64_256
+                if "c3_512" in forms:
+                    forms[key]["over_fp64_single_cube_512"] = forms[key]["value"] / forms["c3_512"]["fp64"]["value"]
     if rank != 0:
         return
 
@@ -443,6 +590,7 @@ def ours(args, rank: int, world: int, local_rank: int):
     bytes_launch = (80 + 120 + 120) / 3 * cells             # compulsory W read + accumulator traffic
     traffic = None if SWEEP_DRAM_BYTES_PER_CELL is None else SWEEP_DRAM_BYTES_PER_CELL * cells
     peak = fp32_peak if prec else fp64_peak
+    hbm_gbs, hbm_src = hbm_peak()
 
     line = {"metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -455,19 +603,18 @@ def ours(args, rank: int, world: int, local_rank: int):
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": traffic if not prec else None, "flops_per_cell_update": flops_cell,
                          "peak_source": "FMA probe run by this bench (gkm_probe_fma_peak)",
-                         "hbm": {"achieved_gbs": bytes_launch / launch_s / 1e9, "peak_gbs": HBM_PEAK_GBS,
-                                 "frac": bytes_launch / launch_s / 1e9 / HBM_PEAK_GBS,
-                                 "peak_source": "measured copy bandwidth"}},
+                         "hbm": {"achieved_gbs": bytes_launch / launch_s / 1e9, "peak_gbs": hbm_gbs,
+                                 "frac": bytes_launch / launch_s / 1e9 / hbm_gbs, "peak_source": hbm_src}},
             "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
             "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, "sweep_shapes": sweep_cfg, "forms": forms}
     if world == 1 and not args.no_cpu_baseline:
-        workers = max(1, min(os.cpu_count() or 1, 8))
-        r = run_reference(workers, 0, 2)
+        # the same measurement as --impl reference: all host cores, the same steps and warm-up
+        workers = max(1, min(os.cpu_count() or 1, 96))
+        r = run_reference(workers, args.warmup, args.steps)
         line["cpu_baseline"] = {"value": r["gcell"], "unit": "Gcell-updates/s", "cores": workers,
                                 "kind": "reference",
-                                "sample": f"{REF_N}^3 cube per process, same recipe, {REF_PART} particles, 2 steps, "
-                                          f"{workers} concurrent processes ({r['wall_s']:.1f} s wall)",
+                                "sample": reference_sample_text(workers, args.warmup, args.steps, r["wall_s"]),
                                 "particle_steps_per_s": r["psteps"]}
     print(json.dumps(line), flush=True)
 
@@ -484,6 +631,10 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed-precision and batched forms")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched ensemble forms")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer plug-point measurement")
+    ap.add_argument("--c2-steps", type=int, default=200,
+                    help="steps of the 256^3 FP64-vs-mixed curve comparison (0 skips it)")
+    ap.add_argument("--c3-steps", type=int, default=500,
+                    help="steps of the 512^3 FP64-vs-mixed run with its error budget (0 skips it)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="form of the main line")
     ap.add_argument("--autotune-reps", type=int, default=2,
                     help="timed launches per sweep shape; 0 keeps the default shapes (profiling runs)")

@@ -14,7 +14,11 @@
 // process exits.  In host code its name only stands for the device object, it
 // is not a device address, so the address is looked up once per device with
 // cudaGetSymbolAddress while that device is current, and that address is what
-// the kernels receive.
+// the kernels receive.  The solver tables are filled by a one-thread kernel on
+// the caller's stream, so a call launches kernels only: no allocation and no
+// host-to-device copy.  All calls share both arrays; calls that overlap on the
+// GPU (on one stream or several) race, so order them on one stream or
+// serialise them.
 #include "gkm.h"
 #include "gkm_internal.h"
 
@@ -42,41 +46,44 @@ DeviceSymbols g_symbols[kMaxDevices];
 // Thomas tables of the line solves: natural dp_1 = 4, m_i = 1/dp_{i-1},
 // dp_i = 4 - m_i; periodic (Sherman-Morrison, gamma = -4) dp_0 = 8,
 // dp_i = b_i - m_i with b_{N-1} = 4.25 and z = B^-1 (-4, 0, .., 0, 1).
-void line_tables(int N, int periodic, std::vector<double>& all, double& denom)
+// One thread fills the table array in device memory, so a call copies nothing
+// from the host; every operation is rounded on its own (no fused multiply-add),
+// which gives the same values as the handle path's host-built tables.
+__global__ void line_tables_kernel(int N, int periodic, double* __restrict__ t)
 {
-    std::vector<double> mt(N + 1, 0.0), dp(N + 1, 0.0), z(N + 1, 0.0);
-    denom = 0.0;
+    double* mt = t;
+    double* dp = t + (N + 1);
+    double* z = t + 2 * (N + 1);
+    for (int i = 0; i <= N; i++) mt[i] = dp[i] = z[i] = 0.0;
     if (!periodic) {
         dp[1] = 4.0;
         for (int i = 2; i <= N - 2; i++) {
-            mt[i] = 1.0 / dp[i - 1];
-            dp[i] = 4.0 - mt[i];
+            mt[i] = __ddiv_rn(1.0, dp[i - 1]);
+            dp[i] = __dsub_rn(4.0, mt[i]);
         }
-    } else {
-        dp[0] = 8.0;
-        for (int i = 1; i < N; i++) {
-            mt[i] = 1.0 / dp[i - 1];
-            dp[i] = ((i == N - 1) ? 4.25 : 4.0) - mt[i];
-        }
-        double rp = -4.0;
-        z[0] = rp;
-        for (int i = 1; i < N; i++) {
-            double r = (i == N - 1) ? 1.0 : 0.0;
-            rp = r - mt[i] * rp;
-            z[i] = rp;
-        }
-        z[N - 1] = z[N - 1] / dp[N - 1];
-        for (int i = N - 2; i >= 0; i--) z[i] = (z[i] - z[i + 1]) / dp[i];
-        denom = 1.0 + (z[0] + (-0.25) * z[N - 1]);
+        return;
     }
-    all.clear();
-    all.insert(all.end(), mt.begin(), mt.end());
-    all.insert(all.end(), dp.begin(), dp.end());
-    all.insert(all.end(), z.begin(), z.end());
+    dp[0] = 8.0;
+    for (int i = 1; i < N; i++) {
+        mt[i] = __ddiv_rn(1.0, dp[i - 1]);
+        dp[i] = __dsub_rn((i == N - 1) ? 4.25 : 4.0, mt[i]);
+    }
+    double rp = -4.0;
+    z[0] = rp;
+    for (int i = 1; i < N; i++) {
+        const double r = (i == N - 1) ? 1.0 : 0.0;
+        rp = __dsub_rn(r, __dmul_rn(mt[i], rp));
+        z[i] = rp;
+    }
+    z[N - 1] = __ddiv_rn(z[N - 1], dp[N - 1]);
+    for (int i = N - 2; i >= 0; i--) z[i] = __ddiv_rn(__dsub_rn(z[i], z[i + 1]), dp[i]);
 }
 
 // Once per device, with that device current: the device addresses of the two
-// static arrays.  The first call on a device performs this lookup.
+// static arrays.  The first call on a device performs this lookup and the
+// addresses are kept for the life of the process; they stay valid as long as
+// the device's primary context does, so a caller that destroys it
+// (cudaDeviceReset) must not call this entry point afterwards.
 cudaError_t device_symbols(DeviceSymbols& out)
 {
     int dev = 0;
@@ -122,11 +129,16 @@ extern "C" gkm_status gkm_spline_build_noalloc(const double* W, int32_t n, int32
     cudaError_t e = device_symbols(sym);
     if (e != cudaSuccess) return GKM_ERR_CUDA;
 
-    std::vector<double> tab;
+    // the periodic Sherman-Morrison denominator is a kernel argument: the host computes it with the
+    // same recurrences (it only needs the scalars, nothing is copied to the device)
     double denom = 0.0;
-    line_tables((int)N, periodic, tab, denom);
+    if (periodic) {
+        std::vector<double> mt(N + 1), dp(N + 1), z(N + 1);
+        gkm::spline_line_tables((int)N, periodic, mt.data(), dp.data(), z.data(), &denom);
+    }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    e = cudaMemcpyAsync(sym.tables, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, s);
+    line_tables_kernel<<<1, 1, 0, s>>>((int)N, periodic, sym.tables);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return GKM_ERR_CUDA;
 
     gkm::FieldConst fc{};

@@ -220,10 +220,13 @@ gkm_status gkm_stats_compute(gkm_handle* h, gkm_stats* out);
  * 24 KiB of solver tables) that every GPU loading the library holds until
  * exit; grids needing more (natural_ghost3: about n > 150) return
  * GKM_ERR_CONFIG with a message on stderr.  The first call on a device looks
- * up that array's device address, so make it before any stream capture.
- * Calls share the array: calls that overlap on the GPU race.  Nothing in the
- * array needs clearing; every element is written before it is read.
- * Results equal gkm_generate_splines + gkm_spline_coefs bit for bit. */
+ * up that array's device address (kept until exit, so do not call it after
+ * cudaDeviceReset), so make it before any stream capture.  The solver tables
+ * are filled on the device: a call launches kernels and copies nothing.
+ * Calls share the array and the tables: calls that overlap on the GPU race,
+ * on one stream or several, so order them on one stream or serialise them.
+ * Nothing in the array needs clearing; every element is written before it is
+ * read.  Results equal gkm_generate_splines + gkm_spline_coefs bit for bit. */
 gkm_status gkm_spline_build_noalloc(const double* W, int32_t n, int32_t spline_mode, int32_t component,
                                     double* coefs, void* stream);
 

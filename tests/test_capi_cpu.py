@@ -101,3 +101,18 @@ def test_ensemble_and_new_entry_points_reject_bad_arguments_without_gpu():
     assert L.gkm_particle_stats_compute(None, None) == _capi.GKM_ERR_ARG
     assert L.gkm_set_pipeline(None, 32, 2) == _capi.GKM_ERR_ARG
     assert L.gkm_spline_build_noalloc(None, 16, 0, 1, None, None) != _capi.GKM_OK
+
+
+def test_reference_gpu_build_exports_the_plug_point():
+    """The reference's -D UseGPU build linked with dns_gkm_lpt_b200/plug/GPUupdate_b200.cpp loads
+    (its libgkm_b200.so dependency resolves) and defines evolve(ptype*[5], DevAlloc*, ptype) and
+    DevAlloc's constructor and destructor (src/GPUupdate.h:33, src/GPUAlloc.h:8-26)."""
+    import ctypes
+    import subprocess
+    so = os.path.join(ROOT, "oracle", "_ref", "libgkm_ref_gpu.so")
+    if not os.path.exists(so):
+        pytest.skip("oracle/_ref/libgkm_ref_gpu.so is built by `make -C oracle` where the reference tree exists")
+    ctypes.CDLL(so)
+    syms = subprocess.run(["nm", "-D", "--defined-only", so], capture_output=True, text=True, check=True).stdout
+    for s in ("_Z6evolvePPdP8DevAllocd", "_ZN8DevAllocC1Ev", "_ZN8DevAllocD1Ev", "gkmrefgpu_setup", "gkmrefgpu_run"):
+        assert f" {s}\n" in syms, s
