@@ -29,7 +29,7 @@ EXPORTS = [
     "gkm_ensemble_member", "gkm_ensemble_step", "gkm_ensemble_step_timed", "gkm_ensemble_autotune",
     "gkm_ensemble_sweep_config", "gkm_ensemble_launch_count", "gkm_ensemble_synchronize", "gkm_ensemble_stream",
     "gkm_particle_props", "gkm_particle_stats_compute", "gkm_write_field", "gkm_write_particles", "gkm_write_time",
-    "gkm_write_reinit", "gkm_set_pipeline",
+    "gkm_write_reinit", "gkm_set_pipeline", "gkm_ensemble_segments",
 ]
 
 PROP_COUNT = 41
@@ -48,7 +48,8 @@ class GkmParams(C.Structure):
 class GkmConfig(C.Structure):
     _fields_ = [("params", GkmParams), ("cfl", C.c_double), ("visc_law", C.c_int32), ("spline_mode", C.c_int32),
                 ("precision", C.c_int32), ("device", C.c_int32), ("max_particles", C.c_int64),
-                ("use_graphs", C.c_int32), ("spline_build", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("use_graphs", C.c_int32), ("spline_build", C.c_int32), ("test_wait_probe", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 class GkmParticleStats(C.Structure):
@@ -120,6 +121,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.gkm_ensemble_step_timed.argtypes = [_h, C.c_int32, C.c_int32, _dp]
     L.gkm_ensemble_autotune.argtypes = [_h, C.c_int32]
     L.gkm_ensemble_sweep_config.argtypes = [_h, C.POINTER(C.c_int32)]
+    L.gkm_ensemble_segments.argtypes = [_h, C.POINTER(C.c_int32), C.c_int64]
     L.gkm_ensemble_launch_count.argtypes = [_h, C.POINTER(C.c_int64)]
     L.gkm_ensemble_synchronize.argtypes = [_h]
     L.gkm_ensemble_stream.argtypes = [_h, C.POINTER(C.c_void_p)]

@@ -151,6 +151,7 @@ cudaError_t launch_sweep_any(gkm_handle* h, int dir, gkm::SweepArgs a)
     const SweepChoice& c = h->sweep[dir];
     a.seg_len = c.seg_len;
     a.tmap = sweep_tmap(h, a.W, dir, c.variant);
+    a.wait_probe = h->cfg.test_wait_probe;
     if (h->cfg.precision == GKM_PREC_MIXED) return gkm::launch_sweep_mixed(dir, c.variant, a, c.nseg, h->stream);
     return gkm::launch_sweep(dir, c.variant, a, c.nseg, h->stream);
 }
@@ -451,6 +452,7 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
     if (cfg->precision < GKM_PREC_FP64 || cfg->precision > GKM_PREC_MIXED || cfg->max_particles < 0)
         return GKM_ERR_CONFIG;
     if (cfg->spline_build < 0 || cfg->spline_build > 2) return GKM_ERR_CONFIG;
+    if (cfg->test_wait_probe < 0 || cfg->test_wait_probe > 1) return GKM_ERR_CONFIG;
     const int K = (int)((5.0 - 3.0 * P.gam) / (P.gam - 1.0));   // src/FlowField.cpp:42
     if (K < 0) return GKM_ERR_CONFIG;
 

@@ -8,8 +8,16 @@
 // item to (member, local item) by binary search over the offsets.  The
 // per-member arithmetic is the single-cube device code, so each member evolves
 // exactly as it would alone.
+//
+// Sweeps: one window variant per direction for all members (one launch has one
+// block shape), and a segment length per member (the autotuner picks one per
+// grid size: short segments give many items, long ones load fewer extra slabs
+// and compute fewer extra faces).  The work list holds the members with the
+// longest items first and the persistent CTAs take items from a counter, so
+// the short items fill the end of the launch.
 #include "gkm_handle.h"
 
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -20,7 +28,9 @@ using gkm::MemberDev;
 namespace {
 
 // offset arrays in d_off, each nm + 1 long longs
-enum OffsetSet { kItemX = 0, kItemY, kItemZ, kGhost, kLine0, kLine1, kWarp2, kPart, kNumSets };
+// kOrderX..Z hold, per sweep direction, the member at each position of the work list
+enum OffsetSet { kItemX = 0, kItemY, kItemZ, kGhost, kLine0, kLine1, kWarp2, kPart, kOrderX, kOrderY, kOrderZ,
+                 kNumSets };
 
 }  // namespace
 
@@ -30,7 +40,9 @@ struct gkm_ensemble {
     bool mixed = false;
     int device = 0;
     cudaStream_t stream = nullptr;
-    SweepChoice sweep[3];                 // variant and segment length shared by all members
+    SweepChoice sweep[3];                 // window variant shared by all members (seg_len unused)
+    std::vector<int> seg[3];              // segment length of each member, per direction
+    unsigned long long* d_next = nullptr; // work counters of the three sweep launches
     MemberDev* d_mem = nullptr;
     long long* d_off = nullptr;
     std::vector<long long> h_off;         // kNumSets x (nm + 1), as last uploaded
@@ -88,6 +100,7 @@ gkm_status refresh(gkm_ensemble* E, bool need_state)
     }
     std::vector<MemberDev> hm((size_t)nm);
     std::vector<long long> off((size_t)kNumSets * (nm + 1), 0);
+    std::vector<std::vector<long long>> items(3, std::vector<long long>((size_t)nm, 0));
     auto at = [&](int set, int m) -> long long& { return off[(size_t)set * (nm + 1) + m]; };
     for (int m = 0; m < nm; m++) {
         const gkm_handle* h = E->mem[m];
@@ -100,12 +113,14 @@ gkm_status refresh(gkm_ensemble* E, bool need_state)
         md.dt_fixed_mode = h->dt_fixed_mode;
         md.dt_fixed = h->dt_fixed;
         const long long n = h->fc.n;
-        long long items[3];
         for (int d = 0; d < 3; d++) {
             const gkm::SweepShape sh = gkm::sweep_shape(E->mixed, E->sweep[d].variant);
-            md.nseg[d] = (int)((n + E->sweep[d].seg_len - 1) / E->sweep[d].seg_len);
+            int L = E->seg[d][(size_t)m];
+            L = L < 1 ? 1 : (L > n ? (int)n : L);
+            md.seg_len[d] = L;
+            md.nseg[d] = (int)((n + L - 1) / L);
             md.tiles_b[d] = (int)((n + sh.TB - 1) / sh.TB);
-            items[d] = (long long)md.tiles_b[d] * ((n + sh.TA - 1) / sh.TA) * md.nseg[d];
+            items[(size_t)d][(size_t)m] = (long long)md.tiles_b[d] * ((n + sh.TA - 1) / sh.TA) * md.nseg[d];
         }
         md.grid = h->grid;
         const int N1 = h->grid.npts + 1;
@@ -120,15 +135,27 @@ gkm_status refresh(gkm_ensemble* E, bool need_state)
         const long long N = h->grid.npts, M = N + h->grid.pad;
         const long long nt = h->fc.nt;
         const bool parts = h->np > 0;   // members without particles skip the spline work
-        const long long count[kNumSets] = {items[0],
-                                           items[1],
-                                           items[2],
-                                           nt * nt * nt - n * n * n,
-                                           parts ? 3 * N * N : 0,
-                                           parts ? 3 * M * N : 0,
-                                           parts ? 3 * ((M * M + 31) / 32) : 0,
-                                           h->np};
-        for (int s = 0; s < kNumSets; s++) at(s, m + 1) = at(s, m) + count[s];
+        const long long count[kPart + 1] = {0,
+                                            0,
+                                            0,
+                                            nt * nt * nt - n * n * n,
+                                            parts ? 3 * N * N : 0,
+                                            parts ? 3 * M * N : 0,
+                                            parts ? 3 * ((M * M + 31) / 32) : 0,
+                                            h->np};
+        for (int s = kGhost; s <= kPart; s++) at(s, m + 1) = at(s, m) + count[s];
+    }
+    // sweep work lists: members in decreasing segment length (longest items first; a stable order,
+    // so equal lengths keep the members' order), offsets by position
+    for (int d = 0; d < 3; d++) {
+        std::vector<int> ord((size_t)nm);
+        for (int m = 0; m < nm; m++) ord[(size_t)m] = m;
+        std::stable_sort(ord.begin(), ord.end(),
+                         [&](int x, int y) { return hm[(size_t)x].seg_len[d] > hm[(size_t)y].seg_len[d]; });
+        for (int p = 0; p < nm; p++) {
+            at(kOrderX + d, p) = ord[(size_t)p];
+            at(kItemX + d, p + 1) = at(kItemX + d, p) + items[(size_t)d][(size_t)ord[(size_t)p]];
+        }
     }
     ECK(E, cudaMemcpyAsync(E->d_mem, hm.data(), sizeof(MemberDev) * (size_t)nm, cudaMemcpyHostToDevice, E->stream));
     if (off != E->h_off) {
@@ -146,10 +173,10 @@ cudaError_t launch_sweep_dir(gkm_ensemble* E, int d, int parity)
     const SweepChoice& c = E->sweep[d];
     E->launches += 1;
     if (E->mixed)
-        return gkm::launch_ensemble_sweep32(d, c.variant, E->d_mem, off_ptr(E, kItemX + d), nm_of(E), parity,
-                                            c.seg_len, E->stream);
-    return gkm::launch_ensemble_sweep64(d, c.variant, E->d_mem, off_ptr(E, kItemX + d), nm_of(E), parity, c.seg_len,
-                                        E->stream);
+        return gkm::launch_ensemble_sweep32(d, c.variant, E->d_mem, off_ptr(E, kItemX + d), off_ptr(E, kOrderX + d),
+                                            nm_of(E), parity, E->d_next + d, E->stream);
+    return gkm::launch_ensemble_sweep64(d, c.variant, E->d_mem, off_ptr(E, kItemX + d), off_ptr(E, kOrderX + d),
+                                        nm_of(E), parity, E->d_next + d, E->stream);
 }
 
 cudaError_t launch_halo_all(gkm_ensemble* E, int parity)
@@ -248,7 +275,10 @@ gkm_status gkm_ensemble_create(const gkm_config* members, int32_t n_members, gkm
     for (int d = 0; d < 3; d++) {
         E->sweep[d].variant = 0;
         E->sweep[d].seg_len = max_n < 16 ? max_n : 16;
+        E->seg[d].assign((size_t)n_members, E->sweep[d].seg_len);
     }
+    e = cudaMalloc(&E->d_next, 3 * sizeof(unsigned long long));
+    if (e != cudaSuccess) return bail(ecuda(E, e, "cudaMalloc(work counters)"));
     e = cudaMalloc(&E->d_mem, sizeof(MemberDev) * (size_t)n_members);
     if (e != cudaSuccess) return bail(ecuda(E, e, "cudaMalloc(members)"));
     e = cudaMalloc(&E->d_off, sizeof(long long) * (size_t)kNumSets * (n_members + 1));
@@ -270,6 +300,7 @@ gkm_status gkm_ensemble_destroy(gkm_ensemble* E)
     for (double* p : E->extra_scratch) cudaFree(p);
     cudaFree(E->d_mem);
     cudaFree(E->d_off);
+    cudaFree(E->d_next);
     if (E->stream) cudaStreamDestroy(E->stream);
     delete E;
     return GKM_OK;
@@ -369,12 +400,19 @@ gkm_status gkm_ensemble_autotune(gkm_ensemble* E, int32_t reps)
         ECK(E, cudaMemcpyAsync(&saved[(size_t)m], E->mem[m]->clock, sizeof(DevClock), cudaMemcpyDeviceToHost,
                                E->stream));
     ECK(E, cudaStreamSynchronize(E->stream));
-    int max_n = 0;
-    for (const gkm_handle* h : E->mem) max_n = h->fc.n > max_n ? h->fc.n : max_n;
-    std::vector<int> lens;
-    for (int L : {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256})
-        if (L < max_n) lens.push_back(L);
-    lens.push_back(max_n);
+    // grid sizes of the members, largest first, and the candidate segment lengths
+    std::vector<int> sizes;
+    for (const gkm_handle* h : E->mem)
+        if (std::find(sizes.begin(), sizes.end(), h->fc.n) == sizes.end()) sizes.push_back(h->fc.n);
+    std::sort(sizes.begin(), sizes.end(), std::greater<int>());
+    auto lens_upto = [](int n) {
+        std::vector<int> v;
+        for (int L : {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256})
+            if (L < n) v.push_back(L);
+        v.push_back(n);
+        return v;
+    };
+    const std::vector<int> lens = lens_upto(sizes[0]);
     const int nvar = E->mixed ? gkm::kSweepVariants32 : gkm::kSweepVariants64;
     const int p = E->mem[0]->parity;
     cudaEvent_t e0, e1;
@@ -382,32 +420,59 @@ gkm_status gkm_ensemble_autotune(gkm_ensemble* E, int32_t reps)
     ECK(E, cudaEventCreate(&e1));
     gkm_status st = GKM_OK;
     const int64_t launches0 = E->launches;
+    // time of `reps` launches of direction d with the current shapes (one untimed launch first)
+    auto time_dir = [&](int d, float* ms) -> gkm_status {
+        gkm_status r = refresh(E, true);
+        if (r != GKM_OK) return r;
+        cudaError_t e = launch_sweep_dir(E, d, p);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, E->stream);
+        for (int k = 0; k < reps && e == cudaSuccess; k++) e = launch_sweep_dir(E, d, p);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, E->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+        return e == cudaSuccess ? GKM_OK : ecuda(E, e, "gkm_ensemble_autotune");
+    };
     for (int d = 0; d < 3 && st == GKM_OK; d++) {
-        SweepChoice best = E->sweep[d];
+        // 1. the window variant, with one segment length for every member
+        int best_v = E->sweep[d].variant, best_L = E->sweep[d].seg_len;
         float best_ms = 1e30f;
         for (int v = 0; v < nvar && st == GKM_OK; v++)
             for (int L : lens) {
                 E->sweep[d].variant = v;
-                E->sweep[d].seg_len = L;
-                st = refresh(E, true);
-                if (st != GKM_OK) break;
-                cudaError_t e = launch_sweep_dir(E, d, p);   // warm-up
-                if (e == cudaSuccess) e = cudaEventRecord(e0, E->stream);
-                for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch_sweep_dir(E, d, p);
-                if (e == cudaSuccess) e = cudaEventRecord(e1, E->stream);
-                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                E->seg[d].assign((size_t)nm, L);
                 float t = 0.f;
-                if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
-                if (e != cudaSuccess) {
-                    st = ecuda(E, e, "gkm_ensemble_autotune");
-                    break;
-                }
+                st = time_dir(d, &t);
+                if (st != GKM_OK) break;
                 if (t < best_ms) {
                     best_ms = t;
-                    best = E->sweep[d];
+                    best_v = v;
+                    best_L = L;
                 }
             }
-        E->sweep[d] = best;
+        E->sweep[d].variant = best_v;
+        E->sweep[d].seg_len = best_L;
+        E->seg[d].assign((size_t)nm, best_L);
+        // 2. one segment length per grid size, largest grids first, the other sizes held
+        for (int n : sizes) {
+            if (st != GKM_OK) break;
+            std::vector<int> keep = E->seg[d];
+            int best_n = -1;
+            for (int L : lens_upto(n)) {
+                for (int m = 0; m < nm; m++)
+                    if (E->mem[m]->fc.n == n) E->seg[d][(size_t)m] = L;
+                float t = 0.f;
+                st = time_dir(d, &t);
+                if (st != GKM_OK) break;
+                if (t < best_ms) {
+                    best_ms = t;
+                    best_n = L;
+                }
+            }
+            E->seg[d] = keep;
+            if (best_n > 0)
+                for (int m = 0; m < nm; m++)
+                    if (E->mem[m]->fc.n == n) E->seg[d][(size_t)m] = best_n;
+        }
     }
     E->launches = launches0;   // tuning launches are not steps
     cudaEventDestroy(e0);
@@ -419,6 +484,19 @@ gkm_status gkm_ensemble_autotune(gkm_ensemble* E, int32_t reps)
     return refresh(E, true);
 }
 
+gkm_status gkm_ensemble_segments(const gkm_ensemble* E, int32_t* out, int64_t capacity)
+{
+    if (!E || !out) return GKM_ERR_ARG;
+    const int nm = nm_of(E);
+    if (capacity < 3LL * nm) return GKM_ERR_ARG;
+    for (int d = 0; d < 3; d++)
+        for (int m = 0; m < nm; m++) {
+            const int n = E->mem[m]->fc.n, L = E->seg[d][(size_t)m];
+            out[(size_t)d * nm + m] = L > n ? n : L;
+        }
+    return GKM_OK;
+}
+
 gkm_status gkm_ensemble_sweep_config(const gkm_ensemble* E, int32_t out[12])
 {
     if (!E || !out) return GKM_ERR_ARG;
@@ -427,7 +505,8 @@ gkm_status gkm_ensemble_sweep_config(const gkm_ensemble* E, int32_t out[12])
         out[4 * d + 0] = E->sweep[d].variant;
         out[4 * d + 1] = sh.TB;
         out[4 * d + 2] = sh.TA;
-        out[4 * d + 3] = E->sweep[d].seg_len;
+        out[4 * d + 3] = E->sweep[d].seg_len;   // the length shared before per-size tuning
+
     }
     return GKM_OK;
 }

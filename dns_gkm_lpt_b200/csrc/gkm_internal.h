@@ -83,6 +83,7 @@ struct SweepArgs {
                                     // at f1 (f0 = f1 = 0: the whole normal range)
     int skip_clock_init;            // 1: the clock's dt and next wave slot were set before the launch
     const void* tmap;               // FP64 x / y sweeps: tensor map of W for the slab copies (else null)
+    int wait_probe;                 // test hook: make CTA (0, 0, 0)'s first bounded copy wait run out
 };
 
 // kernel launchers (sweep.cu); sweep_prepare sets the sweep kernels' shared-memory limit once
@@ -182,6 +183,7 @@ struct MemberDev {
     int dt_fixed_mode;
     double dt_fixed;
     int nseg[3];         // sweep segments along the normal, per direction
+    int seg_len[3];      // faces per segment along the normal, per direction (chosen per member size)
     int tiles_b[3];      // windows along the first in-plane axis, per direction
     SplineGrid grid;
     SplineTables tb;
@@ -215,10 +217,15 @@ __device__ __forceinline__ int find_member(const long long* __restrict__ off, in
     return lo;
 }
 
-cudaError_t launch_ensemble_sweep64(int dir, int variant, const MemberDev* mem, const long long* off, int nm,
-                                    int parity, int seg_len, cudaStream_t s);
-cudaError_t launch_ensemble_sweep32(int dir, int variant, const MemberDev* mem, const long long* off, int nm,
-                                    int parity, int seg_len, cudaStream_t s);
+// One sweep direction over all members: off[] are the prefix offsets of the members' work items in
+// the order order[] (position -> member); CTAs fetch items from *next (zero before the launch), so
+// the list is taken in order, its longest items first when order[] sorts them so.
+cudaError_t launch_ensemble_sweep64(int dir, int variant, const MemberDev* mem, const long long* off,
+                                    const long long* order, int nm, int parity, unsigned long long* next,
+                                    cudaStream_t s);
+cudaError_t launch_ensemble_sweep32(int dir, int variant, const MemberDev* mem, const long long* off,
+                                    const long long* order, int nm, int parity, unsigned long long* next,
+                                    cudaStream_t s);
 cudaError_t launch_ensemble_halo(const MemberDev* mem, const long long* off, int nm, long long total, int buf,
                                  int finish_step, cudaStream_t s);
 cudaError_t launch_ensemble_splines(const MemberDev* mem, const EnsembleWork& w, const long long totals[3], int nm,

@@ -191,11 +191,13 @@ cudaError_t sweep_prepare()
     return e;
 }
 
-cudaError_t launch_ensemble_sweep64(int dir, int variant, const MemberDev* mem, const long long* off, int nm,
-                                    int parity, int seg_len, cudaStream_t s)
+cudaError_t launch_ensemble_sweep64(int dir, int variant, const MemberDev* mem, const long long* off,
+                                    const long long* order, int nm, int parity, unsigned long long* next,
+                                    cudaStream_t s)
 {
-    if (variant == 1) return launch_ensemble_sweep_t<double, SweepTile64b>(dir, mem, off, nm, parity, seg_len, s);
-    return launch_ensemble_sweep_t<double, SweepTile64a>(dir, mem, off, nm, parity, seg_len, s);
+    if (variant == 1)
+        return launch_ensemble_sweep_t<double, SweepTile64b>(dir, mem, off, order, nm, parity, next, s);
+    return launch_ensemble_sweep_t<double, SweepTile64a>(dir, mem, off, order, nm, parity, next, s);
 }
 
 cudaError_t launch_ensemble_halo(const MemberDev* mem, const long long* off, int nm, long long total, int buf,

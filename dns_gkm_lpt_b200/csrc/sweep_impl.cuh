@@ -192,9 +192,9 @@ __device__ __forceinline__ void tma_slab_load(unsigned dst, const void* tmap, in
         "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(0), "r"(bar)
         : "memory");
 }
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, int polls = 1 << 24)
 {
-    for (int it = 0; it < (1 << 24); it++) {
+    for (int it = 0; it < polls; it++) {
         unsigned done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -206,6 +206,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
     return false;
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// retire `bytes` of a barrier phase's expected transaction count without a copy (the failure-detection
+// test hook takes back the bytes it added beyond what its copy delivers)
+__device__ __forceinline__ void mbar_complete_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+// the test hook's extra expected bytes and its short poll count
+constexpr unsigned kProbeExtraBytes = 16;
+constexpr int kProbePolls = 256;
 
 }  // namespace sweep_detail
 
@@ -297,6 +306,10 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     // window, a box of the (k, i, j, q) tensor whose smem image is the slot's [q][a][b] layout)
     // with one bulk tensor copy completing on the mbarrier
     const bool use_tma = !kMixed && DIR != 2 && a.tmap != nullptr;
+    // failure-detection test hook: the first CTA's first copy is expected with kProbeExtraBytes more
+    // than it delivers, so its first wait (kProbePolls polls) runs out and raises status bit 1; the
+    // CTA then retires the extra bytes and waits for the copy itself, which lands normally
+    const bool probe = use_tma && a.wait_probe && bx == 0 && by == 0 && bz == 0;
     const unsigned bar_u32 = smem_u32(bar);
     unsigned tma_phase = 0;
     if (use_tma) {
@@ -372,6 +385,10 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             load_slab(f + 3);
         } else {
             if (use_tma) {
+                if (probe && f == f_begin) {
+                    if (!mbar_wait_bounded(bar_u32, tma_phase, kProbePolls)) atomicOr(&a.clock->status, 2);
+                    if (tid == 0) mbar_complete_tx(bar_u32, kProbeExtraBytes);
+                }
                 if (!mbar_wait_bounded(bar_u32, tma_phase)) atomicOr(&a.clock->status, 2);
                 tma_phase ^= 1u;
             } else {
@@ -482,7 +499,9 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                     // box origin: window row a0-1, column b0-1 (ghost-layout +3), normal plane f+4
                     const int cb = b0 + 2, ca = a0 + 2, cn = f + 4 + 3;
                     tma_slab_load(smem_u32(slot(f + 4)), a.tmap, cb, DIR == 0 ? cn : ca, DIR == 0 ? ca : cn,
-                                  (unsigned)(5 * kWC * sizeof(double)), bar_u32);
+                                  (unsigned)(5 * kWC * sizeof(double)) +
+                                      ((probe && f == f_begin - 1) ? kProbeExtraBytes : 0u),
+                                  bar_u32);
                 }
             } else {
                 issue_slab(f + 4);
@@ -589,20 +608,30 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepA
     sweep_block<DIR, T, Tile>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
 }
 
-// Persistent form for an ensemble: a fixed grid of CTAs walks the flattened
-// (member, window, segment) work list of one sweep direction.  Every member
-// uses segments of seg_len faces; off[] are the members' work-item offsets.
+// Persistent form for an ensemble: a fixed grid of CTAs takes the flattened
+// (member, window, segment) work list of one sweep direction item by item from
+// a global counter, so a CTA that finishes early takes the next item.  Member
+// m uses segments of md.seg_len[DIR] faces; the list holds the members in the
+// order order[] (longest items first), off[] their work-item offsets.
 template <int DIR, class T, class Tile>
 __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
-    ensemble_sweep_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off, int nm, int parity,
-                          int seg_len)
+    ensemble_sweep_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off,
+                          const long long* __restrict__ order, int nm, int parity, unsigned long long* next)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ long long s_item;
     const long long total = off[nm];
-    for (long long item = blockIdx.x; item < total; item += gridDim.x) {
-        const int m = find_member(off, nm, item);
-        const MemberDev& md = mem[m];
-        const long long local = item - off[m];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (;;) {
+        // the previous item ended with a barrier, so every thread has read s_item before it changes
+        if (tid == 0) s_item = (long long)atomicAdd(next, 1ull);
+        __syncthreads();
+        const long long item = s_item;
+        if (item >= total) break;
+        const int pos = find_member(off, nm, item);
+        const MemberDev& md = mem[order[pos]];
+        const int seg_len = md.seg_len[DIR];
+        const long long local = item - off[pos];
         const int nseg = md.nseg[DIR];
         const int tb = md.tiles_b[DIR];
         const int bz = (int)(local % nseg);
@@ -617,6 +646,7 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
         a.f0 = 0;
         a.f1 = 0;
         a.skip_clock_init = 0;
+        a.wait_probe = 0;
         a.W = md.buf[parity];
         a.A = md.buf[parity ^ 1];
         a.fc = md.fc;
@@ -656,20 +686,22 @@ cudaError_t launch_sweep_rows_t(int dir, SweepArgs a, int j0, int j1, cudaStream
 }
 
 template <class T, class Tile>
-cudaError_t launch_ensemble_sweep_t(int dir, const MemberDev* mem, const long long* off, int nm, int parity,
-                                    int seg_len, cudaStream_t s)
+cudaError_t launch_ensemble_sweep_t(int dir, const MemberDev* mem, const long long* off, const long long* order, int nm,
+                                    int parity, unsigned long long* next, cudaStream_t s)
 {
     const dim3 block(Tile::TB, Tile::TA);
     const int grid = 148 * Tile::ctas;
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
     if (dir == 0)
         ensemble_sweep_kernel<0, T, Tile>
-            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 0>(), s>>>(mem, off, nm, parity, seg_len);
+            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 0>(), s>>>(mem, off, order, nm, parity, next);
     else if (dir == 1)
         ensemble_sweep_kernel<1, T, Tile>
-            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 1>(), s>>>(mem, off, nm, parity, seg_len);
+            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 1>(), s>>>(mem, off, order, nm, parity, next);
     else
         ensemble_sweep_kernel<2, T, Tile>
-            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 2>(), s>>>(mem, off, nm, parity, seg_len);
+            <<<grid, block, sweep_detail::sweep_smem_bytes<T, Tile, 2>(), s>>>(mem, off, order, nm, parity, next);
     return cudaGetLastError();
 }
 

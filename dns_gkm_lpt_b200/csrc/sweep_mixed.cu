@@ -40,11 +40,12 @@ cudaError_t sweep_mixed_prepare()
     return e;
 }
 
-cudaError_t launch_ensemble_sweep32(int dir, int variant, const MemberDev* mem, const long long* off, int nm,
-                                    int parity, int seg_len, cudaStream_t s)
+cudaError_t launch_ensemble_sweep32(int dir, int variant, const MemberDev* mem, const long long* off,
+                                    const long long* order, int nm, int parity, unsigned long long* next,
+                                    cudaStream_t s)
 {
     (void)variant;
-    return launch_ensemble_sweep_t<float, SweepTile32a>(dir, mem, off, nm, parity, seg_len, s);
+    return launch_ensemble_sweep_t<float, SweepTile32a>(dir, mem, off, order, nm, parity, next, s);
 }
 
 cudaError_t launch_sweep_mixed_rows(int dir, int variant, SweepArgs a, int j0, int j1, cudaStream_t s)

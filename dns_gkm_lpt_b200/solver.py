@@ -56,7 +56,7 @@ def _w5(W):
 
 def make_config(params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
                 max_particles: int = 0, device: int = 0, use_graphs: bool = True,
-                precision: int = 0, spline_build: int = 0) -> _capi.GkmConfig:
+                precision: int = 0, spline_build: int = 0, test_wait_probe: int = 0) -> _capi.GkmConfig:
     L = _capi.lib()
     cfg = _capi.GkmConfig()
     L.gkm_config_default(C.byref(cfg))
@@ -70,18 +70,19 @@ def make_config(params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mod
     cfg.use_graphs = 1 if use_graphs else 0
     cfg.precision = precision   # 0 FP64, 1 mixed (FP32 reconstruction + flux, FP64 state)
     cfg.spline_build = spline_build   # 0 auto, 1 one component per launch, 2 three components per launch
+    cfg.test_wait_probe = test_wait_probe   # failure-detection test hook (gkm.h), 0 in normal use
     return cfg
 
 
 class Solver:
     def __init__(self, params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
                  max_particles: int = 0, device: int = 0, use_graphs: bool = True, precision: int = 0,
-                 spline_build: int = 0, _member_handle=None):
+                 spline_build: int = 0, test_wait_probe: int = 0, _member_handle=None):
         self.L = _capi.lib()
         self._owned = _member_handle is None
         if self._owned:
             cfg = make_config(params, cfl, visc_law, spline_mode, max_particles, device, use_graphs, precision,
-                              spline_build)
+                              spline_build, test_wait_probe)
             h = C.c_void_p()
             s = self.L.gkm_create(C.byref(cfg), C.byref(h))
             if s != 0:
@@ -328,8 +329,22 @@ class Ensemble:
     def sweep_config(self) -> list:
         out = (C.c_int32 * 12)()
         self._check(self.L.gkm_ensemble_sweep_config(self.h, out))
-        return [{"dir": "xyz"[d], "variant": out[4 * d], "window": [out[4 * d + 1], out[4 * d + 2]],
-                 "segment": out[4 * d + 3]} for d in range(3)]
+        segs = self.segments()
+        cfg = []
+        for d in range(3):
+            by_n = {}
+            for m, L in enumerate(segs[d]):
+                by_n[self.members[m].n] = L
+            cfg.append({"dir": "xyz"[d], "variant": out[4 * d], "window": [out[4 * d + 1], out[4 * d + 2]],
+                        "segment": out[4 * d + 3], "segment_by_grid_size": dict(sorted(by_n.items()))})
+        return cfg
+
+    def segments(self) -> list:
+        """Segment length of every member, per sweep direction: [x list, y list, z list]."""
+        nm = len(self)
+        out = (C.c_int32 * (3 * nm))()
+        self._check(self.L.gkm_ensemble_segments(self.h, out, 3 * nm))
+        return [[out[d * nm + m] for m in range(nm)] for d in range(3)]
 
     def launch_count(self) -> int:
         n = C.c_int64()

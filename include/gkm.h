@@ -81,7 +81,14 @@ typedef struct gkm_config {
     int32_t spline_build;    /* velocity splines: 0 auto, 1 one component per launch, 2 each pass
                                 for all three components in one launch (two more scratch
                                 arrays; auto picks it for grids up to about 440^3); same bits */
-    int32_t reserved[6];
+    int32_t test_wait_probe; /* failure-detection test hook (no reference counterpart), 0 = off.
+                                1: in every FP64 x / y sweep launch that lands its slabs by bulk
+                                tensor copy, the first CTA arms its first copy's barrier with 16
+                                bytes more than the copy delivers and polls it 256 times, so that
+                                bounded wait runs out and raises the status the host reports as
+                                GKM_ERR_CUDA; the CTA then retires the extra bytes and waits for
+                                the copy, so results are unchanged and nothing stays in flight */
+    int32_t reserved[5];
 } gkm_config;
 
 /* One PrintStats line (src/update.cpp:835-840), field part. */
@@ -333,12 +340,19 @@ gkm_status gkm_ensemble_step(gkm_ensemble* e, int32_t nsteps, int32_t with_parti
  * steps: ms[0..2] x/y/z sweeps, ms[3] ghost wrap, ms[4] splines,
  * ms[5] particles, ms[6] whole steps. */
 gkm_status gkm_ensemble_step_timed(gkm_ensemble* e, int32_t nsteps, int32_t with_particles, double ms[7]);
-/* Times every window variant x segment length of each sweep direction over
- * the whole ensemble (reps launches each) and keeps the fastest; the state is
- * untouched and every member's clock is restored. */
+/* Per sweep direction, times over the whole ensemble (reps launches each):
+ * every window variant with one segment length for all members, then, for
+ * each grid size in turn (largest first), every segment length for the
+ * members of that size; keeps the fastest.  The state is untouched and every
+ * member's clock is restored.  A sweep launch takes the members with the
+ * longest segments first. */
 gkm_status gkm_ensemble_autotune(gkm_ensemble* e, int32_t reps);
-/* out[4d..4d+3] = window variant, window width, window height, segment length */
+/* out[4d..4d+3] = window variant, window width, window height, and the
+ * segment length the variant was chosen with (before the per-size lengths) */
 gkm_status gkm_ensemble_sweep_config(const gkm_ensemble* e, int32_t out[12]);
+/* Segment length of every member per direction: out[d * n_members + m]
+ * (capacity >= 3 x n_members).  No reference counterpart. */
+gkm_status gkm_ensemble_segments(const gkm_ensemble* e, int32_t* out, int64_t capacity);
 gkm_status gkm_ensemble_launch_count(const gkm_ensemble* e, int64_t* count);
 gkm_status gkm_ensemble_synchronize(gkm_ensemble* e);
 /* The ensemble's stream (cudaStream_t as void*), for events or interop. */

