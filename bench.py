@@ -51,9 +51,9 @@ REF_PART = N_PART * REF_N ** 3 // N_CELLS ** 3   # same particle density
 C3_PART = 4_000_000          # particles of the 512^3 mixed-precision case
 HBM_FALLBACK_GBS = 6650.0    # an earlier copy-bandwidth measurement on these B200s, used only without a
                              # measured-peaks file beside this script
-# DRAM bytes per cell of one sweep launch, from the ncu capture of a 128^3 case (traffic scales with
-# the cells a launch processes; mean over the x, y, z sweeps)
-SWEEP_DRAM_BYTES_PER_CELL = 97.9   # mean DRAM bytes per cell of the x, y, z sweep launches (ncu, 128^3)
+# DRAM bytes per cell of one sweep launch: mean over the x, y, z sweeps of the ncu capture of this
+# benchmark's 256^3 cube (83.8, 123.3, 141.4 B; compulsory 80, 120, 120)
+SWEEP_DRAM_BYTES_PER_CELL = 116.2
 
 
 def hbm_peak():
@@ -111,13 +111,14 @@ def case_of(n: int):
     return SIZES.get(n, (MT, RE))
 
 
-def workload(n=N_CELLS, npart=N_PART, precision="fp64"):
+def workload(n=N_CELLS, npart=N_PART, precision="fp64", spline_precision="fp64"):
     Mt, Re = case_of(n)
     form = {"fp64": "FP64 drop-in", "mixed": "mixed precision (FP32 WENO + flux, FP64 state)"}.get(
         precision, "FP64 drop-in and mixed precision from the same field")
     nt = n + 6
+    spl = "natural_ghost3 splines" + (", FP32 velocity-spline coefficients" if spline_precision == "fp32" else "")
     return {"workload": f"{n}^3 periodic cube, {form}, Mt {Mt}, Re_lambda {Re:g}, {npart} particles, "
-                        f"cfl {CFL}, natural_ghost3 splines",
+                        f"cfl {CFL}, {spl}",
             "n": n, "particles": npart, "cfl": CFL, "precision": precision, "seed": SEED,
             "l2": f"no flush: resident state 2 x {5 * nt ** 3 * 8 / 1e9:.2f} GB exceeds the 126 MB L2",
             "parallelism": "replicas"}
@@ -452,7 +453,15 @@ def ours(args, rank: int, world: int, local_rank: int):
 
     fp64_peak, fp32_peak = probe_fma_peak(local_rank)
     stream = torch.cuda.Stream()
-    s = Solver(P, cfl=CFL, max_particles=npart, device=local_rank, precision=prec)
+    sp32 = args.spline_precision == "fp32"
+    free0 = torch.cuda.mem_get_info(local_rank)[0]
+    s = Solver(P, cfl=CFL, max_particles=npart, device=local_rank, precision=prec, spline_precision=1 if sp32 else 0)
+    free1 = torch.cuda.mem_get_info(local_rank)[0]
+    Ms = (n + 6) + 2   # natural_ghost3 spline grid: N = n + 6 points, N + 2 coefficients per axis
+    memory = {"handle_bytes": free0 - free1,
+              "spline_coefficient_bytes": 3 * Ms ** 3 * (4 if sp32 else 8),
+              "spline_scratch_bytes": Ms * Ms * (n + 6) * 8,
+              "spline_coefficient_bytes_fp64": 3 * Ms ** 3 * 8}
     s.set_stream(stream.cuda_stream)
     s.upload_state(W0)
     s.particles_upload(pos0)
@@ -596,8 +605,9 @@ def ours(args, rank: int, world: int, local_rank: int):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec else "f64",
             "data": "synthetic: seeded solenoidal field (init_DNS recipe), uniform particles",
-            "config": workload(n, npart, args.precision),
+            "config": workload(n, npart, args.precision, args.spline_precision),
             "particle_steps_per_s": world * npart * args.steps / (part_ms * 1e-3),
+            "memory": memory,
             "phases_ms_per_step": {k: v / args.steps for k, v in ph.items()},
             "roofline": {"kernel": "sweep_kernel (x/y/z, one launch each per step)", "bound": "fp32" if prec else "fp64",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
@@ -636,6 +646,8 @@ def main():
     ap.add_argument("--c3-steps", type=int, default=500,
                     help="steps of the 512^3 FP64-vs-mixed run with its error budget (0 skips it)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="form of the main line")
+    ap.add_argument("--spline-precision", default="fp64", choices=["fp64", "fp32"],
+                    help="velocity-spline coefficients of the main line (fp32: same FP64 solves, stored rounded)")
     ap.add_argument("--autotune-reps", type=int, default=2,
                     help="timed launches per sweep shape; 0 keeps the default shapes (profiling runs)")
     args = ap.parse_args()

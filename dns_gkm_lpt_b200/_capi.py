@@ -49,7 +49,7 @@ class GkmConfig(C.Structure):
     _fields_ = [("params", GkmParams), ("cfl", C.c_double), ("visc_law", C.c_int32), ("spline_mode", C.c_int32),
                 ("precision", C.c_int32), ("device", C.c_int32), ("max_particles", C.c_int64),
                 ("use_graphs", C.c_int32), ("spline_build", C.c_int32), ("test_wait_probe", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("spline_precision", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class GkmParticleStats(C.Structure):

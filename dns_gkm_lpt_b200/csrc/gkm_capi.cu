@@ -194,6 +194,11 @@ cudaError_t enqueue_eulerian(gkm_handle* h)
 
 cudaError_t enqueue_splines(gkm_handle* h, const double* W)
 {
+    if (h->spline_f32) {
+        h->launches += kSplinePasses;
+        return gkm::launch_spline_build_f32(W, h->fc, h->grid, device_tables(h), h->coef32[0], h->coef32[1],
+                                            h->coef32[2], h->scratch, h->stream);
+    }
     if (h->d_self && (W == h->buf[0] || W == h->buf[1])) {
         gkm::EnsembleWork w{};
         w.line0 = h->d_self_off;
@@ -213,7 +218,7 @@ cudaError_t enqueue_splines(gkm_handle* h, const double* W)
 cudaError_t setup_batched_splines(gkm_handle* h)
 {
     const long long N = h->grid.npts, M = N + h->grid.pad;
-    if (h->cfg.spline_build == 1) return cudaSuccess;
+    if (h->cfg.spline_build == 1 || h->spline_f32) return cudaSuccess;
     if (h->cfg.spline_build == 0 && 3 * N * N > 2LL * 148 * 2048) return cudaSuccess;
     const size_t scratch_bytes = sizeof(double) * (size_t)(M * M * N);
     size_t free_b = 0, total_b = 0;
@@ -263,8 +268,13 @@ cudaError_t enqueue_advect(gkm_handle* h)
                                               h->stream);
     h->launches += nl + 1;
     if (e != cudaSuccess) return e;
-    const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
     h->launches += 1;
+    if (h->spline_f32) {
+        const float* c32[3] = {h->coef32[0], h->coef32[1], h->coef32[2]};
+        return gkm::launch_particles_heun(c32, h->grid, h->clock, h->np, arrays_of(h->P_sorted), arrays_of(h->P),
+                                          h->tag_sorted, h->tag, h->stream);
+    }
+    const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
     return gkm::launch_particles_heun(c, h->grid, h->clock, h->np, arrays_of(h->P_sorted), arrays_of(h->P),
                                       h->tag_sorted, h->tag, h->stream);
 }
@@ -373,6 +383,8 @@ gkm_status host_tags(gkm_handle* h, std::vector<long long>& tags)
 // (src/ParticleTrack.cpp:99-113) into h->props; allocates on first use
 gkm_status compute_props(gkm_handle* h)
 {
+    if (h->spline_f32)
+        return fail(h, GKM_ERR_CONFIG, "particle properties need FP64 velocity-spline coefficients");
     gkm_status s = ensure_splines(h);
     if (s != GKM_OK) return s;
     const long long M = h->grid.npts + h->grid.pad;
@@ -453,6 +465,8 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
         return GKM_ERR_CONFIG;
     if (cfg->spline_build < 0 || cfg->spline_build > 2) return GKM_ERR_CONFIG;
     if (cfg->test_wait_probe < 0 || cfg->test_wait_probe > 1) return GKM_ERR_CONFIG;
+    if (cfg->spline_precision < GKM_SPLINE_COEF_FP64 || cfg->spline_precision > GKM_SPLINE_COEF_FP32)
+        return GKM_ERR_CONFIG;
     const int K = (int)((5.0 - 3.0 * P.gam) / (P.gam - 1.0));   // src/FlowField.cpp:42
     if (K < 0) return GKM_ERR_CONFIG;
 
@@ -535,8 +549,10 @@ gkm_status gkm_create(const gkm_config* cfg, gkm_handle** out)
         if (e != cudaSuccess) return bail(e, "cudaMemcpy(tables)");
     }
     const long long M = h->grid.npts + h->grid.pad, N = h->grid.npts;
+    h->spline_f32 = cfg->spline_precision == GKM_SPLINE_COEF_FP32;
     for (int c = 0; c < 3; c++) {
-        e = cudaMalloc(&h->coef[c], sizeof(double) * (size_t)(M * M * M));
+        if (h->spline_f32) e = cudaMalloc(&h->coef32[c], sizeof(float) * (size_t)(M * M * M));
+        else e = cudaMalloc(&h->coef[c], sizeof(double) * (size_t)(M * M * M));
         if (e != cudaSuccess) return bail(e, "cudaMalloc(spline coefficients)");
     }
     e = cudaMalloc(&h->scratch, sizeof(double) * (size_t)(M * M * N));
@@ -581,7 +597,10 @@ gkm_status gkm_destroy(gkm_handle* h)
     for (int b = 0; b < 2; b++) cudaFree(h->buf[b]);
     cudaFree(h->clock);
     cudaFree(h->tables);
-    for (int c = 0; c < 3; c++) cudaFree(h->coef[c]);
+    for (int c = 0; c < 3; c++) {
+        cudaFree(h->coef[c]);
+        cudaFree(h->coef32[c]);
+    }
     cudaFree(h->scratch);
     for (int k = 0; k < 2; k++) cudaFree(h->scratch_extra[k]);
     cudaFree(h->d_self);
@@ -1073,9 +1092,14 @@ gkm_status gkm_particles_upload(gkm_handle* h, int64_t np, const double* pos, co
         gkm_status s = ensure_splines(h);
         if (s != GKM_OK) return s;
         const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+        const float* c32[3] = {h->coef32[0], h->coef32[1], h->coef32[2]};
         h->launches += 1;
-        CK(h, gkm::launch_particles_eval(c, h->grid, np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4], h->P[5],
-                                         h->stream));
+        if (h->spline_f32)
+            CK(h, gkm::launch_particles_eval(c32, h->grid, np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4], h->P[5],
+                                             h->stream));
+        else
+            CK(h, gkm::launch_particles_eval(c, h->grid, np, h->P[0], h->P[1], h->P[2], h->P[3], h->P[4], h->P[5],
+                                             h->stream));
     }
     return GKM_OK;
 }
@@ -1112,6 +1136,13 @@ gkm_status gkm_spline_coefs(gkm_handle* h, int32_t c, double* out, int64_t capac
     if (capacity < coef_count(h)) return fail(h, GKM_ERR_ARG, "capacity below (N+P)^3");
     gkm_status s = ensure_splines(h);
     if (s != GKM_OK) return s;
+    if (h->spline_f32) {   // the stored floats, widened
+        std::vector<float> tmp((size_t)coef_count(h));
+        CK(h, cudaMemcpyAsync(tmp.data(), h->coef32[c], sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < tmp.size(); i++) out[i] = (double)tmp[i];
+        return GKM_OK;
+    }
     CK(h, cudaMemcpyAsync(out, h->coef[c], sizeof(double) * (size_t)coef_count(h), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     return GKM_OK;
@@ -1124,8 +1155,14 @@ gkm_status gkm_stats_compute(gkm_handle* h, gkm_stats* out)
     gkm_status s = ensure_splines(h);
     if (s != GKM_OK) return s;
     const double* c[3] = {h->coef[0], h->coef[1], h->coef[2]};
+    const float* c32[3] = {h->coef32[0], h->coef32[1], h->coef32[2]};
     h->launches += 4;
-    CK(h, gkm::launch_stats(h->buf[h->parity], h->fc, h->grid, c, h->partials, kStatsBlocks, h->stats_out, h->stream));
+    if (h->spline_f32)
+        CK(h, gkm::launch_stats(h->buf[h->parity], h->fc, h->grid, c32, h->partials, kStatsBlocks, h->stats_out,
+                                h->stream));
+    else
+        CK(h, gkm::launch_stats(h->buf[h->parity], h->fc, h->grid, c, h->partials, kStatsBlocks, h->stats_out,
+                                h->stream));
     double v[32];
     CK(h, cudaMemcpyAsync(v, h->stats_out, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
     DevClock ck;

@@ -241,6 +241,8 @@ gkm_status gkm_ensemble_create(const gkm_config* members, int32_t n_members, gkm
     for (int m = 1; m < n_members; m++)
         if (members[m].device != members[0].device || members[m].precision != members[0].precision)
             return GKM_ERR_CONFIG;
+    for (int m = 0; m < n_members; m++)   // the ensemble's spline kernels store FP64 coefficients
+        if (members[m].spline_precision != GKM_SPLINE_COEF_FP64) return GKM_ERR_CONFIG;
     gkm_ensemble* E = new gkm_ensemble();
     E->mixed = members[0].precision == GKM_PREC_MIXED;
     E->device = members[0].device;

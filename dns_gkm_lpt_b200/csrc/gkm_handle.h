@@ -31,6 +31,8 @@ struct gkm_handle {
     double* tables = nullptr;  // mt | dp | z, each npts+1
     double denom = 0.0;
     double* coef[3] = {nullptr, nullptr, nullptr};
+    float* coef32[3] = {nullptr, nullptr, nullptr};   // GKM_SPLINE_COEF_FP32: the coefficients, rounded
+    bool spline_f32 = false;
     double* scratch = nullptr;
     // the three velocity splines built together (one launch per pass for all three components):
     // two more scratch arrays and a one-member descriptor for the ensemble spline kernels;

@@ -142,10 +142,21 @@ cudaError_t launch_spline_component(const double* W, const FieldConst& fc, const
 cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np,
                                   const double* py, const double* px, const double* pz,
                                   double* Uu, double* Uv, double* Uw, cudaStream_t s);
+// FP32 velocity splines: the three components' coefficients rounded to float after the same FP64
+// line solves (buf: M^2 N doubles, the handle's spline scratch); evaluation reads them as floats
+// and computes in FP64
+cudaError_t launch_spline_build_f32(const double* W, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
+                                    float* coef_u, float* coef_v, float* coef_w, double* buf, cudaStream_t s);
+cudaError_t launch_particles_eval(const float* const coefs[3], const SplineGrid& g, long long np,
+                                  const double* py, const double* px, const double* pz,
+                                  double* Uu, double* Uv, double* Uw, cudaStream_t s);
 struct ParticleArrays {   // y, x, z, u, v, w
     double* a[6];
 };
 cudaError_t launch_particles_heun(const double* const coefs[3], const SplineGrid& g, const DevClock* clock,
+                                  long long np, const ParticleArrays& src, const ParticleArrays& dst,
+                                  const long long* tag_src, long long* tag_dst, cudaStream_t s);
+cudaError_t launch_particles_heun(const float* const coefs[3], const SplineGrid& g, const DevClock* clock,
                                   long long np, const ParticleArrays& src, const ParticleArrays& dst,
                                   const long long* tag_src, long long* tag_dst, cudaStream_t s);
 // order the particles of src by blocks of 8^3 spline cells into dst (tags move with them);
@@ -170,6 +181,8 @@ cudaError_t launch_particle_props(const double* const coefs[8], const SplineGrid
 cudaError_t launch_particle_stats(const double* props, long long np, StatsPartial* partials, int nblocks, double* out6,
                                   cudaStream_t s);
 cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const double* const coefs[3],
+                         StatsPartial* partials, int nblocks, double* out16, cudaStream_t s);
+cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const float* const coefs[3],
                          StatsPartial* partials, int nblocks, double* out16, cudaStream_t s);
 
 // ---------------------------------------------------------------- ensemble --

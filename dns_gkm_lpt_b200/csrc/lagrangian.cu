@@ -125,6 +125,98 @@ __device__ void line_solve(const Src& f, int N, int periodic, const SplineTables
     }
 }
 
+// line_solve with the intermediate results stored one slot lower (the forward value of point i in
+// slot i, where the input of point i was), so the line may be solved in place: c may be the
+// storage f reads (same stride), as long as slots N .. N+pad-1 exist past the N inputs.  The
+// arithmetic and its order are those of line_solve, so the coefficients are identical.
+template <int U, class Src>
+__device__ void line_solve_ip(const Src& f, int N, int periodic, const SplineTables& tb, double* c, long long cs)
+{
+    if (!periodic) {
+        const double c0 = f(0), cl = f(N - 1);
+        double rp = 0.0;
+        auto fwd = [&](int i, double fi) {
+            double r = mul(6.0, fi);
+            if (i == 1) r = sub(r, c0);
+            if (i == N - 2) r = sub(r, cl);
+            rp = (i == 1) ? r : sub(r, mul(tb.mt[i], rp));
+            c[(long long)i * cs] = rp;
+        };
+        int i = 1;
+        for (; i + U - 1 <= N - 2; i += U) {
+            double fv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) fv[u] = f(i + u);
+#pragma unroll
+            for (int u = 0; u < U; u++) fwd(i + u, fv[u]);
+        }
+        for (; i <= N - 2; i++) fwd(i, f(i));
+        double x = __ddiv_rn(c[(long long)(N - 2) * cs], tb.dp[N - 2]);
+        c[(long long)(N - 1) * cs] = x;
+        i = N - 3;
+        for (; i - U + 1 >= 1; i -= U) {
+            double cv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) cv[u] = c[(long long)(i - u) * cs];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                x = __ddiv_rn(sub(cv[u], x), tb.dp[i - u]);
+                c[(long long)(i - u + 1) * cs] = x;
+            }
+        }
+        for (; i >= 1; i--) {
+            x = __ddiv_rn(sub(c[(long long)i * cs], x), tb.dp[i]);
+            c[(long long)(i + 1) * cs] = x;
+        }
+        const double x1 = (N - 2 >= 1) ? c[2 * cs] : cl;
+        const double xl2 = (N - 2 >= 1) ? c[(long long)(N - 1) * cs] : c0;
+        c[cs] = c0;
+        c[(long long)N * cs] = cl;
+        c[0] = sub(2.0 * c0, x1);
+        c[(long long)(N + 1) * cs] = sub(2.0 * cl, xl2);
+    } else {
+        double rp = mul(6.0, f(0));
+        c[0] = rp;
+        int i = 1;
+        for (; i + U - 1 <= N - 1; i += U) {
+            double fv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) fv[u] = f(i + u);
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                rp = sub(mul(6.0, fv[u]), mul(tb.mt[i + u], rp));
+                c[(long long)(i + u) * cs] = rp;
+            }
+        }
+        for (; i < N; i++) {
+            rp = sub(mul(6.0, f(i)), mul(tb.mt[i], rp));
+            c[(long long)i * cs] = rp;
+        }
+        double x = __ddiv_rn(c[(long long)(N - 1) * cs], tb.dp[N - 1]);
+        c[(long long)N * cs] = x;
+        i = N - 2;
+        for (; i - U + 1 >= 0; i -= U) {
+            double cv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) cv[u] = c[(long long)(i - u) * cs];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                x = __ddiv_rn(sub(cv[u], x), tb.dp[i - u]);
+                c[(long long)(i - u + 1) * cs] = x;
+            }
+        }
+        for (; i >= 0; i--) {
+            x = __ddiv_rn(sub(c[(long long)i * cs], x), tb.dp[i]);
+            c[(long long)(i + 1) * cs] = x;
+        }
+        const double fac = __ddiv_rn(add(c[cs], mul(-0.25, c[(long long)N * cs])), tb.denom);
+        for (int i = 0; i < N; i++) c[(long long)(i + 1) * cs] = sub(c[(long long)(i + 1) * cs], mul(fac, tb.z[i]));
+        c[0] = c[(long long)N * cs];
+        c[(long long)(N + 1) * cs] = c[cs];
+        c[(long long)(N + 2) * cs] = c[2 * cs];
+    }
+}
+
 // Data of a spline at ghost-layout cell idx (generateSplines, src/update.cpp:1200-1210,1239-1241):
 // q = 1..3 velocity rho u_q / rho; q = kSrcDensity rho; q = kSrcPressure
 // (rho (gam-1)) (rho E / rho - |u|^2 / 2); q = kSrcPlain the array itself (one nt^3 component).
@@ -144,10 +236,11 @@ __device__ __forceinline__ double spline_source(const double* __restrict__ W, lo
 // pass 0: the data of source q along axis 0 (y) -> out [M0][N1][N2]; one line (i, k)
 template <int U>
 __device__ __forceinline__ void pass0_line(const double* __restrict__ W, const FieldConst& fc, const SplineGrid& g,
-                                           const SplineTables& tb, int q, double* __restrict__ out, long long L)
+                                           const SplineTables& tb, int q, double* __restrict__ out, long long L,
+                                           long long stride = 0)
 {
     const int N = g.npts;
-    const long long lines = (long long)N * N;
+    const long long lines = stride ? stride : (long long)N * N;   // output stride along axis 0
     const long long nt3 = fc.nt3;
     const int nt = fc.nt;
     const int off = g.periodic ? 3 : 0;
@@ -326,6 +419,175 @@ __global__ void __launch_bounds__(32 * kPass2Warps) spline_pass2(const double* _
         pass2_group(in, g, tb, out, L0, lines, stage[warp]);
 }
 
+// ---- velocity splines with FP32 coefficients: the same FP64 line solves, only the stored
+// coefficients are rounded to single precision.  Pass 0 writes [M0][M1][N2] with room along axis
+// 1, pass 1 solves in place there, pass 2 solves each of its lines in place and writes the rounded
+// coefficients: one FP64 buffer of M^2 N values serves all three components (instead of that
+// scratch plus three FP64 coefficient arrays of M^3).
+__global__ void spline_pass0_room(const double* __restrict__ W, FieldConst fc, SplineGrid g, SplineTables tb, int q,
+                                  double* __restrict__ out)
+{
+    const long long lines = (long long)g.npts * g.npts;
+    const long long stride = (long long)(g.npts + g.pad) * g.npts;
+    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x)
+        pass0_line<kLineBatchSingle>(W, fc, g, tb, q, out, L, stride);
+}
+
+// pass 1 in place on [M0][M1][N2]: line (a, k) reads rows 0..N-1 and writes rows 0..M-1
+__global__ void spline_pass1_inplace(double* buf, SplineGrid g, SplineTables tb)
+{
+    const int N = g.npts, M = N + g.pad;
+    const long long lines = (long long)M * N;
+    for (long long L = blockIdx.x * (long long)blockDim.x + threadIdx.x; L < lines; L += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(L / N), k = (int)(L - (long long)a * N);
+        double* line = buf + (long long)a * M * N + k;
+        auto f = [&](int i) { return line[(long long)i * N]; };
+        line_solve_ip<kLineBatchSingle>(f, N, g.periodic, tb, line, N);
+    }
+}
+
+// pass 2 with FP32 output: the lines of [M0][M1][N2] along axis 2, 32 per warp through shared
+// memory as pass2_group, the forward values stored in the line's own slots (slot i); natural ends:
+// the backward sweep writes each solution rounded as its coefficient; periodic: the solution of
+// point i goes to slot i+1 (i <= N-2; the last one stays in a register) for the correction sweep,
+// which writes the rounded coefficients.  Output [M0][M1][M2] floats.
+__device__ __forceinline__ void pass2_group_f32(double* in, const SplineGrid& g, const SplineTables& tb,
+                                                float* __restrict__ out, long long L0, long long lines,
+                                                double (*sm)[kLineChunk + 1])
+{
+    const int N = g.npts, M = N + g.pad;
+    const int lane = threadIdx.x & 31;
+    const int nl = (int)min(32LL, lines - L0);
+    const long long myL = L0 + lane;
+    const bool mine = lane < nl;
+    auto load = [&](int k0) {
+        for (int j = 0; j < nl; j++) {
+            const int k = k0 + lane;
+            if (k < N) sm[j][lane] = in[(L0 + j) * N + k];
+        }
+        __syncwarp();
+    };
+    // staged values of points k (k < kmax) into slots k + off of their lines
+    auto store = [&](int k0, int off, int kmax) {
+        __syncwarp();
+        for (int j = 0; j < nl; j++) {
+            const int k = k0 + lane;
+            if (k < kmax) in[(L0 + j) * N + k + off] = sm[j][lane];
+        }
+        __syncwarp();
+    };
+    // staged values of slots k (kmin <= k < kmax) rounded into coefficients k + off
+    auto emit = [&](int k0, int kmin, int kmax, int off) {
+        __syncwarp();
+        for (int j = 0; j < nl; j++) {
+            const int k = k0 + lane;
+            if (k >= kmin && k < kmax) out[(L0 + j) * M + k + off] = (float)sm[j][lane];
+        }
+        __syncwarp();
+    };
+    const double* src = in + myL * N;
+    float* dst = out + myL * M;
+    const int top = ((N - 1) / kLineChunk) * kLineChunk;
+    if (!g.periodic) {
+        const double c0 = mine ? src[0] : 0.0, cl = mine ? src[N - 1] : 0.0;
+        double rp = 0.0;
+        for (int k0 = 0; k0 < N; k0 += kLineChunk) {
+            load(k0);
+            if (mine)
+                for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
+                    const int i = k0 + t;
+                    if (i < 1 || i > N - 2) continue;
+                    double r = mul(6.0, sm[lane][t]);
+                    if (i == 1) r = sub(r, c0);
+                    if (i == N - 2) r = sub(r, cl);
+                    rp = (i == 1) ? r : sub(r, mul(tb.mt[i], rp));
+                    sm[lane][t] = rp;
+                }
+            store(k0, 0, N);
+        }
+        double x = 0.0, x1 = 0.0, xl2 = 0.0;
+        for (int k0 = top; k0 >= 0; k0 -= kLineChunk) {
+            load(k0);
+            if (mine)
+                for (int t = kLineChunk - 1; t >= 0; t--) {
+                    const int i = k0 + t;
+                    if (i < 1 || i > N - 2) continue;
+                    x = (i == N - 2) ? __ddiv_rn(sm[lane][t], tb.dp[N - 2]) : __ddiv_rn(sub(sm[lane][t], x), tb.dp[i]);
+                    sm[lane][t] = x;
+                    if (i == N - 2) xl2 = x;
+                    if (i == 1) x1 = x;
+                }
+            emit(k0, 1, N - 1, 1);   // the solution of point i is coefficient i + 1 (1 <= i <= N-2)
+        }
+        if (mine) {
+            dst[1] = (float)c0;
+            dst[0] = (float)sub(2.0 * c0, x1);
+            dst[N] = (float)cl;
+            dst[N + 1] = (float)sub(2.0 * cl, xl2);
+        }
+    } else {
+        double rp = 0.0;
+        for (int k0 = 0; k0 < N; k0 += kLineChunk) {
+            load(k0);
+            if (mine)
+                for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
+                    const int i = k0 + t;
+                    rp = (i == 0) ? mul(6.0, sm[lane][t]) : sub(mul(6.0, sm[lane][t]), mul(tb.mt[i], rp));
+                    sm[lane][t] = rp;
+                }
+            store(k0, 0, N);
+        }
+        double x = 0.0, x0 = 0.0, xl = 0.0;
+        for (int k0 = top; k0 >= 0; k0 -= kLineChunk) {
+            load(k0);
+            if (mine)
+                for (int t = kLineChunk - 1; t >= 0; t--) {
+                    const int i = k0 + t;
+                    if (i > N - 1) continue;
+                    x = (i == N - 1) ? __ddiv_rn(sm[lane][t], tb.dp[N - 1]) : __ddiv_rn(sub(sm[lane][t], x), tb.dp[i]);
+                    sm[lane][t] = x;
+                    if (i == N - 1) xl = x;
+                    if (i == 0) x0 = x;
+                }
+            store(k0, 1, N - 1);
+        }
+        const double fac = mine ? __ddiv_rn(add(x0, mul(-0.25, xl)), tb.denom) : 0.0;
+        double y0 = 0.0, y1 = 0.0;
+        for (int k0 = 0; k0 < N; k0 += kLineChunk) {
+            load(k0);
+            if (mine)
+                for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
+                    const int s = k0 + t;   // slot s holds point s-1
+                    if (s < 1) continue;
+                    const double v = sub(sm[lane][t], mul(fac, tb.z[s - 1]));
+                    sm[lane][t] = v;
+                    if (s == 1) y0 = v;
+                    if (s == 2) y1 = v;
+                }
+            emit(k0, 1, N, 0);
+        }
+        if (mine) {
+            const double yl = sub(xl, mul(fac, tb.z[N - 1]));
+            dst[N] = (float)yl;
+            dst[0] = (float)yl;
+            dst[N + 1] = (float)y0;
+            dst[N + 2] = (float)y1;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(32 * kPass2Warps) spline_pass2_f32(double* in, SplineGrid g, SplineTables tb,
+                                                                     float* __restrict__ out)
+{
+    __shared__ double stage[kPass2Warps][32][kLineChunk + 1];
+    const int M = g.npts + g.pad;
+    const long long lines = (long long)M * M;
+    const int warp = threadIdx.x >> 5;
+    const long long nwarps = (long long)gridDim.x * kPass2Warps;
+    for (long long L0 = ((long long)blockIdx.x * kPass2Warps + warp) * 32; L0 < lines; L0 += nwarps * 32)
+        pass2_group_f32(in, g, tb, out, L0, lines, stage[warp]);
+}
+
 struct Basis {
     double w[4];
 };
@@ -359,8 +621,11 @@ __device__ __forceinline__ Basis basis(double t)
     return b;
 }
 
-// value of one spline at a point (the oracle's contraction order: z, then x, then y)
-__device__ __forceinline__ double spline_value(const double* __restrict__ C, const SplineGrid& g, int ia, int ib, int ic,
+// value of one spline at a point (the oracle's contraction order: z, then x, then y); CT is the
+// type the coefficients are stored in (double, or float for the FP32 velocity splines), the
+// arithmetic is FP64
+template <class CT>
+__device__ __forceinline__ double spline_value(const CT* __restrict__ C, const SplineGrid& g, int ia, int ib, int ic,
                                                const Basis& A, const Basis& B, const Basis& Cz)
 {
     const long long M = g.npts + g.pad;
@@ -370,9 +635,10 @@ __device__ __forceinline__ double spline_value(const double* __restrict__ C, con
         double bw = 0.0;
 #pragma unroll
         for (int y = 0; y < 4; y++) {
-            const double* row = C + ((long long)(ia + x) * M + (ib + y)) * M + ic;
-            const double cw = add(add(add(mul(Cz.w[0], row[0]), mul(Cz.w[1], row[1])), mul(Cz.w[2], row[2])),
-                                  mul(Cz.w[3], row[3]));
+            const CT* row = C + ((long long)(ia + x) * M + (ib + y)) * M + ic;
+            const double cw = add(add(add(mul(Cz.w[0], (double)row[0]), mul(Cz.w[1], (double)row[1])),
+                                      mul(Cz.w[2], (double)row[2])),
+                                  mul(Cz.w[3], (double)row[3]));
             bw = (y == 0) ? mul(B.w[0], cw) : add(bw, mul(B.w[y], cw));
         }
         v = add(v, mul(A.w[x], bw));
@@ -380,19 +646,22 @@ __device__ __forceinline__ double spline_value(const double* __restrict__ C, con
     return v;
 }
 
-__device__ __forceinline__ void eval3(const double* const* coefs, const SplineGrid& g, double a, double b, double c,
+template <class CT>
+__device__ __forceinline__ void eval3(const CT* const* coefs, const SplineGrid& g, double a, double b, double c,
                                       double out[3])
 {
     double ta, tb, tc;
     const int ia = locate(g, a, ta), ib = locate(g, b, tb), ic = locate(g, c, tc);
     const Basis A = basis(ta), B = basis(tb), Cz = basis(tc);
 #pragma unroll
-    for (int f = 0; f < 3; f++) out[f] = spline_value(coefs[f], g, ia, ib, ic, A, B, Cz);
+    for (int f = 0; f < 3; f++) out[f] = spline_value<CT>(coefs[f], g, ia, ib, ic, A, B, Cz);
 }
 
-struct Coefs3 {
-    const double* c[3];
+template <class CT>
+struct Coefs3T {
+    const CT* c[3];
 };
+using Coefs3 = Coefs3T<double>;
 
 // ---------------------------------------------- values, gradients, Hessians --
 // eval_UBspline_3d_d_vg / _vgl / _vgh as the CPU oracle evaluates them: basis
@@ -597,13 +866,14 @@ __global__ void particle_stats_finish(const StatsPartial* __restrict__ part, int
     out[s] = v;
 }
 
-__global__ void particles_eval_kernel(Coefs3 cf, SplineGrid g, long long np, const double* __restrict__ py,
+template <class CT>
+__global__ void particles_eval_kernel(Coefs3T<CT> cf, SplineGrid g, long long np, const double* __restrict__ py,
                                       const double* __restrict__ px, const double* __restrict__ pz,
                                       double* __restrict__ Uu, double* __restrict__ Uv, double* __restrict__ Uw)
 {
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
         double U[3];
-        eval3(cf.c, g, py[p], px[p], pz[p], U);
+        eval3<CT>(cf.c, g, py[p], px[p], pz[p], U);
         Uu[p] = U[0];
         Uv[p] = U[1];
         Uw[p] = U[2];
@@ -616,14 +886,15 @@ __global__ void particles_eval_kernel(Coefs3 cf, SplineGrid g, long long np, con
 // next step's predictor (the reference's getParticleProp at loop start).
 // particle p read from src and written to dst (the same arrays, or the sorted copy and the
 // particle arrays); arrays y, x, z, u, v, w
-__device__ __forceinline__ void heun_particle(const Coefs3& cf, const SplineGrid& g, double dt, long long p,
+template <class CT>
+__device__ __forceinline__ void heun_particle(const Coefs3T<CT>& cf, const SplineGrid& g, double dt, long long p,
                                               const ParticleArrays& src, const ParticleArrays& dst)
 {
     const double twopi = 2.0 * 3.14159265358979311600;   // 2 * atan(1)*4 in double
     double pos[3] = {src.a[0][p], src.a[1][p], src.a[2][p]};
     const double U[3] = {src.a[3][p], src.a[4][p], src.a[5][p]};
     double U2[3];
-    eval3(cf.c, g, add(pos[0], mul(U[1], dt)), add(pos[1], mul(U[0], dt)), add(pos[2], mul(U[2], dt)), U2);
+    eval3<CT>(cf.c, g, add(pos[0], mul(U[1], dt)), add(pos[1], mul(U[0], dt)), add(pos[2], mul(U[2], dt)), U2);
     pos[0] = add(pos[0], mul(mul(0.5, add(U[1], U2[1])), dt));
     pos[1] = add(pos[1], mul(mul(0.5, add(U[0], U2[0])), dt));
     pos[2] = add(pos[2], mul(mul(0.5, add(U[2], U2[2])), dt));
@@ -633,7 +904,7 @@ __device__ __forceinline__ void heun_particle(const Coefs3& cf, const SplineGrid
         if (pos[q] < 0) pos[q] = sub(twopi, fmod(-pos[q], twopi));
     }
     double Un[3];
-    eval3(cf.c, g, pos[0], pos[1], pos[2], Un);
+    eval3<CT>(cf.c, g, pos[0], pos[1], pos[2], Un);
     dst.a[0][p] = pos[0];
     dst.a[1][p] = pos[1];
     dst.a[2][p] = pos[2];
@@ -647,13 +918,14 @@ __device__ __forceinline__ void heun_particle(const Coefs3& cf, const SplineGrid
 // pos += (U + U2) dt / 2, periodic wrap, then U at the new position for the
 // next step's predictor (the reference's getParticleProp at loop start).
 // With tag_src the particles come from the sorted copy and their tags move with them.
-__global__ void particles_heun_kernel(Coefs3 cf, SplineGrid g, const DevClock* __restrict__ clock, long long np,
+template <class CT>
+__global__ void particles_heun_kernel(Coefs3T<CT> cf, SplineGrid g, const DevClock* __restrict__ clock, long long np,
                                       ParticleArrays src, ParticleArrays dst, const long long* __restrict__ tag_src,
                                       long long* __restrict__ tag_dst)
 {
     const double dt = clock->dt;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
-        heun_particle(cf, g, dt, p, src, dst);
+        heun_particle<CT>(cf, g, dt, p, src, dst);
         if (tag_src) tag_dst[p] = tag_src[p];
     }
 }
@@ -741,7 +1013,8 @@ __global__ void particle_scatter_kernel(long long np, const unsigned* __restrict
 // value equals the data (interpolation), so rho and u come from the cell; the
 // gradients come from the coefficients: per axis the node weights are
 // (1, 4, 1)/6 for values and (-1, 0, 1)/2 * dinv for the derivative.
-__device__ __forceinline__ void node_grad(const double* __restrict__ C, long long M, int a, int b, int c, double dinv,
+template <class CT>
+__device__ __forceinline__ void node_grad(const CT* __restrict__ C, long long M, int a, int b, int c, double dinv,
                                           double g[3])
 {
     const double w[3] = {1.0 / 6.0, 4.0 / 6.0, 1.0 / 6.0};
@@ -751,9 +1024,10 @@ __device__ __forceinline__ void node_grad(const double* __restrict__ C, long lon
     for (int x = 0; x < 3; x++)
 #pragma unroll
         for (int y = 0; y < 3; y++) {
-            const double* row = C + ((long long)(a + x) * M + (b + y)) * M + c;
-            const double cw = w[0] * row[0] + w[1] * row[1] + w[2] * row[2];
-            const double cd = d[0] * row[0] + d[2] * row[2];
+            const CT* row = C + ((long long)(a + x) * M + (b + y)) * M + c;
+            const double r0 = (double)row[0], r1 = (double)row[1], r2 = (double)row[2];
+            const double cw = w[0] * r0 + w[1] * r1 + w[2] * r2;
+            const double cd = d[0] * r0 + d[2] * r2;
             g0 += d[x] * w[y] * cw;
             g1 += w[x] * d[y] * cw;
             g2 += w[x] * w[y] * cd;
@@ -782,8 +1056,8 @@ __device__ __forceinline__ void cell_c2p(const double* W, long long nt3, long lo
     T = P / (287.0 * d);
 }
 
-template <int PASS>
-__global__ void stats_kernel(const double* __restrict__ W, FieldConst fc, SplineGrid g, Coefs3 cf,
+template <int PASS, class CT>
+__global__ void stats_kernel(const double* __restrict__ W, FieldConst fc, SplineGrid g, Coefs3T<CT> cf,
                              const double* __restrict__ means, StatsPartial* __restrict__ part)
 {
     __shared__ double red[16][32];
@@ -801,9 +1075,9 @@ __global__ void stats_kernel(const double* __restrict__ W, FieldConst fc, Spline
         cell_c2p(W, nt3, idx, fc.gm1, d, u, v, w, P, T);
         if (PASS == 0) {
             double gu[3], gv[3], gw[3];
-            node_grad(cf.c[0], M, j + off, i + off, k + off, g.dinv, gu);
-            node_grad(cf.c[1], M, j + off, i + off, k + off, g.dinv, gv);
-            node_grad(cf.c[2], M, j + off, i + off, k + off, g.dinv, gw);
+            node_grad<CT>(cf.c[0], M, j + off, i + off, k + off, g.dinv, gu);
+            node_grad<CT>(cf.c[1], M, j + off, i + off, k + off, g.dinv, gv);
+            node_grad<CT>(cf.c[2], M, j + off, i + off, k + off, g.dinv, gw);
             const double dudx = gu[1], dudy = gu[0], dudz = gu[2];
             const double dvdx = gv[1], dvdy = gv[0], dvdz = gv[2];
             const double dwdx = gw[1], dwdy = gw[0], dwdz = gw[2];
@@ -922,7 +1196,7 @@ __global__ void ensemble_heun_kernel(const MemberDev* __restrict__ mem, const lo
         const MemberDev& md = mem[m];
         const Coefs3 cf{{md.coef[0], md.coef[1], md.coef[2]}};
         const ParticleArrays P{{md.P[0], md.P[1], md.P[2], md.P[3], md.P[4], md.P[5]}};
-        heun_particle(cf, md.grid, md.clock->dt, x - off[m], P, P);
+        heun_particle<double>(cf, md.grid, md.clock->dt, x - off[m], P, P);
     }
 }
 
@@ -1018,22 +1292,52 @@ cudaError_t launch_particle_stats(const double* props, long long np, StatsPartia
     return cudaGetLastError();
 }
 
+template <class CT>
+static cudaError_t particles_eval_t(const CT* const coefs[3], const SplineGrid& g, long long np, const double* py,
+                                    const double* px, const double* pz, double* Uu, double* Uv, double* Uw,
+                                    cudaStream_t s)
+{
+    if (np <= 0) return cudaSuccess;
+    Coefs3T<CT> cf{{coefs[0], coefs[1], coefs[2]}};
+    return grid_launch(particles_eval_kernel<CT>, np, 128, s, cf, g, np, py, px, pz, Uu, Uv, Uw);
+}
+
 cudaError_t launch_particles_eval(const double* const coefs[3], const SplineGrid& g, long long np, const double* py,
                                   const double* px, const double* pz, double* Uu, double* Uv, double* Uw,
                                   cudaStream_t s)
 {
+    return particles_eval_t<double>(coefs, g, np, py, px, pz, Uu, Uv, Uw, s);
+}
+
+cudaError_t launch_particles_eval(const float* const coefs[3], const SplineGrid& g, long long np, const double* py,
+                                  const double* px, const double* pz, double* Uu, double* Uv, double* Uw,
+                                  cudaStream_t s)
+{
+    return particles_eval_t<float>(coefs, g, np, py, px, pz, Uu, Uv, Uw, s);
+}
+
+template <class CT>
+static cudaError_t particles_heun_t(const CT* const coefs[3], const SplineGrid& g, const DevClock* clock, long long np,
+                                    const ParticleArrays& src, const ParticleArrays& dst, const long long* tag_src,
+                                    long long* tag_dst, cudaStream_t s)
+{
     if (np <= 0) return cudaSuccess;
-    Coefs3 cf{{coefs[0], coefs[1], coefs[2]}};
-    return grid_launch(particles_eval_kernel, np, 128, s, cf, g, np, py, px, pz, Uu, Uv, Uw);
+    Coefs3T<CT> cf{{coefs[0], coefs[1], coefs[2]}};
+    return grid_launch(particles_heun_kernel<CT>, np, 128, s, cf, g, clock, np, src, dst, tag_src, tag_dst);
 }
 
 cudaError_t launch_particles_heun(const double* const coefs[3], const SplineGrid& g, const DevClock* clock, long long np,
                                   const ParticleArrays& src, const ParticleArrays& dst, const long long* tag_src,
                                   long long* tag_dst, cudaStream_t s)
 {
-    if (np <= 0) return cudaSuccess;
-    Coefs3 cf{{coefs[0], coefs[1], coefs[2]}};
-    return grid_launch(particles_heun_kernel, np, 128, s, cf, g, clock, np, src, dst, tag_src, tag_dst);
+    return particles_heun_t<double>(coefs, g, clock, np, src, dst, tag_src, tag_dst, s);
+}
+
+cudaError_t launch_particles_heun(const float* const coefs[3], const SplineGrid& g, const DevClock* clock, long long np,
+                                  const ParticleArrays& src, const ParticleArrays& dst, const long long* tag_src,
+                                  long long* tag_dst, cudaStream_t s)
+{
+    return particles_heun_t<float>(coefs, g, clock, np, src, dst, tag_src, tag_dst, s);
 }
 
 int scan_temp_size(long long n)
@@ -1082,17 +1386,50 @@ cudaError_t launch_particle_sort(const SplineGrid& g, long long np, const Partic
     return grid_launch(particle_scatter_kernel, np, 256, s, np, (const unsigned*)keys, counts, src, dst, tag_src, tag_dst);
 }
 
+template <class CT>
+static cudaError_t stats_t(const double* W, const FieldConst& fc, const SplineGrid& g, const CT* const coefs[3],
+                           StatsPartial* partials, int nblocks, double* out, cudaStream_t s)
+{
+    Coefs3T<CT> cf{{coefs[0], coefs[1], coefs[2]}};
+    const double ncells = (double)fc.n * fc.n * fc.n;
+    stats_kernel<0, CT><<<nblocks, 256, 0, s>>>(W, fc, g, cf, nullptr, partials);
+    stats_finish<<<1, 32, 0, s>>>(partials, nblocks, ncells, 0, out);
+    // means of p, T, 1/rho sit in out[12..14]
+    stats_kernel<1, CT><<<nblocks, 256, 0, s>>>(W, fc, g, cf, out + 12, partials);
+    stats_finish<<<1, 32, 0, s>>>(partials, nblocks, ncells, 1, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const double* const coefs[3],
                          StatsPartial* partials, int nblocks, double* out, cudaStream_t s)
 {
-    Coefs3 cf{{coefs[0], coefs[1], coefs[2]}};
-    const double ncells = (double)fc.n * fc.n * fc.n;
-    stats_kernel<0><<<nblocks, 256, 0, s>>>(W, fc, g, cf, nullptr, partials);
-    stats_finish<<<1, 32, 0, s>>>(partials, nblocks, ncells, 0, out);
-    // means of p, T, 1/rho sit in out[12..14]
-    stats_kernel<1><<<nblocks, 256, 0, s>>>(W, fc, g, cf, out + 12, partials);
-    stats_finish<<<1, 32, 0, s>>>(partials, nblocks, ncells, 1, out);
-    return cudaGetLastError();
+    return stats_t<double>(W, fc, g, coefs, partials, nblocks, out, s);
+}
+
+cudaError_t launch_stats(const double* W, const FieldConst& fc, const SplineGrid& g, const float* const coefs[3],
+                         StatsPartial* partials, int nblocks, double* out, cudaStream_t s)
+{
+    return stats_t<float>(W, fc, g, coefs, partials, nblocks, out, s);
+}
+
+cudaError_t launch_spline_build_f32(const double* W, const FieldConst& fc, const SplineGrid& g, const SplineTables& tb,
+                                    float* coef_u, float* coef_v, float* coef_w, double* buf, cudaStream_t s)
+{
+    float* outs[3] = {coef_u, coef_v, coef_w};
+    const long long N = g.npts, M = N + g.pad;
+    for (int f = 0; f < 3; f++) {
+        cudaError_t e = grid_launch(spline_pass0_room, N * N, 128, s, W, fc, g, tb, f + 1, buf);
+        if (e != cudaSuccess) return e;
+        e = grid_launch(spline_pass1_inplace, M * N, 128, s, buf, g, tb);
+        if (e != cudaSuccess) return e;
+        long long b = (M * M + 32 * kPass2Warps - 1) / (32 * kPass2Warps);
+        if (b < 1) b = 1;
+        if (b > 148 * 16) b = 148 * 16;
+        spline_pass2_f32<<<(unsigned)b, 32 * kPass2Warps, 0, s>>>(buf, g, tb, outs[f]);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace gkm

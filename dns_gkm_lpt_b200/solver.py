@@ -56,7 +56,8 @@ def _w5(W):
 
 def make_config(params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
                 max_particles: int = 0, device: int = 0, use_graphs: bool = True,
-                precision: int = 0, spline_build: int = 0, test_wait_probe: int = 0) -> _capi.GkmConfig:
+                precision: int = 0, spline_build: int = 0, test_wait_probe: int = 0,
+                spline_precision: int = 0) -> _capi.GkmConfig:
     L = _capi.lib()
     cfg = _capi.GkmConfig()
     L.gkm_config_default(C.byref(cfg))
@@ -71,18 +72,20 @@ def make_config(params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mod
     cfg.precision = precision   # 0 FP64, 1 mixed (FP32 reconstruction + flux, FP64 state)
     cfg.spline_build = spline_build   # 0 auto, 1 one component per launch, 2 three components per launch
     cfg.test_wait_probe = test_wait_probe   # failure-detection test hook (gkm.h), 0 in normal use
+    cfg.spline_precision = spline_precision   # 0 FP64 velocity-spline coefficients, 1 FP32 (same FP64 solves)
     return cfg
 
 
 class Solver:
     def __init__(self, params: Params, cfl: float = 0.10, visc_law: int = 0, spline_mode: int = 0,
                  max_particles: int = 0, device: int = 0, use_graphs: bool = True, precision: int = 0,
-                 spline_build: int = 0, test_wait_probe: int = 0, _member_handle=None):
+                 spline_build: int = 0, test_wait_probe: int = 0, spline_precision: int = 0,
+                 _member_handle=None):
         self.L = _capi.lib()
         self._owned = _member_handle is None
         if self._owned:
             cfg = make_config(params, cfl, visc_law, spline_mode, max_particles, device, use_graphs, precision,
-                              spline_build, test_wait_probe)
+                              spline_build, test_wait_probe, spline_precision)
             h = C.c_void_p()
             s = self.L.gkm_create(C.byref(cfg), C.byref(h))
             if s != 0:

@@ -50,6 +50,13 @@ typedef enum gkm_spline_mode {
     GKM_SPLINE_PERIODIC = 1        /* n interior cell centres, periodic */
 } gkm_spline_mode;
 
+typedef enum gkm_spline_precision {
+    GKM_SPLINE_COEF_FP64 = 0, /* velocity-spline coefficients stored in FP64 (the reference's double) */
+    GKM_SPLINE_COEF_FP32 = 1  /* the same FP64 line solves, coefficients stored rounded to FP32 and
+                                 read as floats by the tricubic evaluation (FP64 arithmetic): half the
+                                 coefficient memory and gather traffic; no counterpart in the reference */
+} gkm_spline_precision;
+
 typedef enum gkm_precision {
     GKM_PREC_FP64 = 0, /* FP64 everywhere (the reference's ptype = double) */
     GKM_PREC_MIXED = 1 /* WENO + gas-kinetic flux in FP32 on non-dimensional values; BGK time
@@ -88,7 +95,11 @@ typedef struct gkm_config {
                                 bounded wait runs out and raises the status the host reports as
                                 GKM_ERR_CUDA; the CTA then retires the extra bytes and waits for
                                 the copy, so results are unchanged and nothing stays in flight */
-    int32_t reserved[5];
+    int32_t spline_precision; /* gkm_spline_precision.  With FP32 coefficients the splines are built
+                                 one component at a time in one FP64 buffer of (N+P)^2 N values
+                                 (besides the 3 (N+P)^3 floats); particle properties (gkm_particle_props
+                                 and what uses them) need FP64 coefficients and return GKM_ERR_CONFIG */
+    int32_t reserved[4];
 } gkm_config;
 
 /* One PrintStats line (src/update.cpp:835-840), field part. */
