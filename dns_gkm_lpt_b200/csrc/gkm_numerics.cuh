@@ -23,6 +23,7 @@
 #ifdef __CUDACC__
 #include <cuda_runtime.h>
 #define GKM_HD __host__ __device__ __forceinline__
+#include "f32x2.cuh"
 #else
 // host-only compilation (op counting, CPU checks of the device numerics)
 #include <algorithm>
@@ -45,6 +46,18 @@
 #endif
 
 namespace gkm {
+
+// single-precision arithmetic: float, and the packed pair F2 (f32x2.cuh)
+template <class T>
+struct single_t {
+    static constexpr bool value = sizeof(T) == 4;
+};
+#ifdef __CUDACC__
+template <>
+struct single_t<F2> {
+    static constexpr bool value = true;
+};
+#endif
 
 constexpr double kR = 287.0;        // gas constant, src/param.h:21
 constexpr double kPrandtl = 0.70;   // src/param.h:19
@@ -116,7 +129,7 @@ GKM_HD void weno_core(T a3, T a2, T a1, T b1, T b2, T b3, T eps, T& o0, T& o1, T
 #endif
     I3p = fmax(fmax(fmax(I0p, I1p), I2p), I3p);
     I3n = fmax(fmax(fmax(I0n, I1n), I2n), I3n);
-    if constexpr (sizeof(T) == 4) {
+    if constexpr (single_t<T>::value) {
         static_assert(!ND, "the single-precision form has no shared denominators");
         // single precision: products of three (eps + IS) underflow on flat stencils,
         // so form the alphas from reciprocals
@@ -659,8 +672,8 @@ struct Tau {
     T c0[4], cv[4], cw[4], c4[4];   // tau_0, tau_2, tau_3, tau_4 of Q_0 .. Q_3
 };
 
-template <bool ADD, class T>
-GKM_HD void put(T& x, T v)
+template <bool ADD, class T, class V>
+GKM_HD void put(T& x, const V& v)
 {
     if constexpr (ADD) x += v;
     else x = v;
@@ -843,6 +856,80 @@ GKM_HD SlopeState<T> slope_state_prim(const Prim<T>& st, T iK3, int K)
     return s;
 }
 
+// The equilibrium part of the flux (src/GKMflux.cpp:73-229 after the two half-Maxwellians):
+// the equilibrium state We at the face, its slopes from the cell averages and the tangential
+// slopes by_, bz_ the sides gathered, the time derivative from Bacc, and the flux moments added to
+// Facc.  gm1..p2 are the time coefficients of src/GKMflux.cpp:162-167,197-204.
+template <class T, class Prov>
+GKM_HD void gks_equilibrium_part(const Prov& in, const T We[5], const T by_[5], const T bz_[5], T Bacc[5], T Facc[5],
+                                 T gm1, T gm2, T gm3, T p0, T p1, T p2, T iK3, T dx, const Phys<T>& ph, T F[5])
+{
+    const int K = ph.K;
+    T M[5];
+    const Prim<T> ste = prim<T>(We, ph.gm1);
+    const T dene = ste.den;
+    Moments<T> E;
+    build_moments_prim<T>(E, ste, K, +1);
+    // the negative half space of the equilibrium: full table minus the positive half
+    T H2[7];
+#pragma unroll
+    for (int i = 0; i < 7; i++) H2[i] = E.X[i] - E.H[i];
+    SlopeState<T> se = slope_state_prim<T>(ste, iK3, K);
+    Tau<T> tp;
+    T b[5], a[5];
+    const T idx2 = (T(2) / dx) * ste.ir;
+    // normal equilibrium slopes from the cell averages, src/GKMflux.cpp:115-116
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (We[q] - in.WL(q)) * idx2;
+    slope_solve<T>(b, se, a);
+    tau_psi<T>(tp, a, E);
+    contract<1, 0, 2>(M, E.H, tp);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    contract<2, 0, 2>(M, E.H, tp);
+    axpy5<T>(Facc, p2 * dene, M);
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (in.WR(q) - We[q]) * idx2;
+    slope_solve<T>(b, se, a);
+    tau_psi<T>(tp, a, E);
+    contract<1, 0, 2>(M, H2, tp);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    contract<2, 0, 2>(M, H2, tp);
+    axpy5<T>(Facc, p2 * dene, M);
+    // tangential equilibrium slopes: G_E = v (psi.a_y) + w (psi.a_z),
+    //   Q_0 = v R(a_y) + w R(a_z), Q_1 = a1y v + a1z w, Q_2 = (a4y/2) v + (a4z/2) w
+    slope_solve<T>(by_, se, a);
+    {
+        const T h4 = T(0.5) * a[4];
+        tau_R<false, 1, 0, 0>(tp, a, h4, E);
+        tau_mono<false, 1, 0, 1>(tp, a[1], E);
+        tau_mono<false, 1, 0, 2>(tp, h4, E);
+    }
+    slope_solve<T>(bz_, se, a);
+    {
+        const T h4 = T(0.5) * a[4];
+        tau_R<true, 0, 1, 0>(tp, a, h4, E);
+        tau_mono<true, 0, 1, 1>(tp, a[1], E);
+        tau_mono<true, 0, 1, 2>(tp, h4, E);
+    }
+    contract<0, 0, 2>(M, E.X, tp);
+    axpy5<T>(Bacc, gm2 * dene, M);
+    contract<1, 0, 2>(M, E.X, tp);
+    axpy5<T>(Facc, p2 * dene, M);
+    // time derivative of the equilibrium, src/GKMflux.cpp:183-191
+    mcal0<0, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
+    const T idene = ste.ir;
+#pragma unroll
+    for (int q = 0; q < 5; q++) b[q] = (gm1 * dene * M[q] + Bacc[q] + gm3 * We[q]) * idene;
+    slope_solve<T>(b, se, a);
+    tau_psi<T>(tp, a, E);
+    contract<1, 0, 2>(M, E.X, tp);
+    axpy5<T>(Facc, p1 * dene, M);
+    mcal0<1, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
+    axpy5<T>(Facc, p0 * dene, M);
+#pragma unroll
+    for (int q = 0; q < 5; q++) F[q] = Facc[q];
+}
+
 // The flux of gks_flux_mcal with the moment functionals above: the same
 // moments of the same slope vectors (src/GKMflux.cpp:11-229), grouped per
 // polynomial instead of per MCal call.
@@ -952,71 +1039,9 @@ GKM_HD void gks_flux_tau(const Prov& in, T tau0, T dt, T dx, const Phys<T>& ph, 
         mcal0<1, 0, 0, T>(M, S.H, GKM_TABLES(S), S.Ie2);
         axpy5<T>(Facc, p3 * den, M);
     }
-
-    // ---------------- equilibrium part
-    const Prim<T> ste = prim<T>(We, ph.gm1);
-    const T dene = ste.den;
-    Moments<T> E;
-    build_moments_prim<T>(E, ste, K, +1);
-    // the negative half space of the equilibrium: full table minus the positive half
-    T H2[7];
-#pragma unroll
-    for (int i = 0; i < 7; i++) H2[i] = E.X[i] - E.H[i];
-    SlopeState<T> se = slope_state_prim<T>(ste, iK3, K);
-    Tau<T> tp;
-    T b[5], a[5];
-    const T idx2 = (T(2) / dx) * ste.ir;
-    // normal equilibrium slopes from the cell averages, src/GKMflux.cpp:115-116
-#pragma unroll
-    for (int q = 0; q < 5; q++) b[q] = (We[q] - in.WL(q)) * idx2;
-    slope_solve<T>(b, se, a);
-    tau_psi<T>(tp, a, E);
-    contract<1, 0, 2>(M, E.H, tp);
-    axpy5<T>(Bacc, gm2 * dene, M);
-    contract<2, 0, 2>(M, E.H, tp);
-    axpy5<T>(Facc, p2 * dene, M);
-#pragma unroll
-    for (int q = 0; q < 5; q++) b[q] = (in.WR(q) - We[q]) * idx2;
-    slope_solve<T>(b, se, a);
-    tau_psi<T>(tp, a, E);
-    contract<1, 0, 2>(M, H2, tp);
-    axpy5<T>(Bacc, gm2 * dene, M);
-    contract<2, 0, 2>(M, H2, tp);
-    axpy5<T>(Facc, p2 * dene, M);
-    // tangential equilibrium slopes: G_E = v (psi.a_y) + w (psi.a_z),
-    //   Q_0 = v R(a_y) + w R(a_z), Q_1 = a1y v + a1z w, Q_2 = (a4y/2) v + (a4z/2) w
-    slope_solve<T>(by_, se, a);
-    {
-        const T h4 = T(0.5) * a[4];
-        tau_R<false, 1, 0, 0>(tp, a, h4, E);
-        tau_mono<false, 1, 0, 1>(tp, a[1], E);
-        tau_mono<false, 1, 0, 2>(tp, h4, E);
-    }
-    slope_solve<T>(bz_, se, a);
-    {
-        const T h4 = T(0.5) * a[4];
-        tau_R<true, 0, 1, 0>(tp, a, h4, E);
-        tau_mono<true, 0, 1, 1>(tp, a[1], E);
-        tau_mono<true, 0, 1, 2>(tp, h4, E);
-    }
-    contract<0, 0, 2>(M, E.X, tp);
-    axpy5<T>(Bacc, gm2 * dene, M);
-    contract<1, 0, 2>(M, E.X, tp);
-    axpy5<T>(Facc, p2 * dene, M);
-    // time derivative of the equilibrium, src/GKMflux.cpp:183-191
-    mcal0<0, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
-    const T idene = ste.ir;
-#pragma unroll
-    for (int q = 0; q < 5; q++) b[q] = (gm1 * dene * M[q] + Bacc[q] + gm3 * We[q]) * idene;
-    slope_solve<T>(b, se, a);
-    tau_psi<T>(tp, a, E);
-    contract<1, 0, 2>(M, E.X, tp);
-    axpy5<T>(Facc, p1 * dene, M);
-    mcal0<1, 0, 0, T>(M, E.X, GKM_TABLES(E), E.Ie2);
-    axpy5<T>(Facc, p0 * dene, M);
-#pragma unroll
-    for (int q = 0; q < 5; q++) F[q] = Facc[q];
+    gks_equilibrium_part<T>(in, We, by_, bz_, Bacc, Facc, gm1, gm2, gm3, p0, p1, p2, iK3, dx, ph, F);
 }
+
 #endif
 
 // The flux the kernels run: the functional form where the tangential product

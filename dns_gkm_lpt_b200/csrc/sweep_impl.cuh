@@ -290,6 +290,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     const T dxw = kMixed ? T(1) : T(fc.dx);
     const T inv_dxw = kMixed ? T(1) : T(fc.inv_dx);
     const Phys<T> ph{T(fc.gam), T(fc.gm1), kMixed ? T(1) : T(kR), fc.K};
+    const float cv_mixed = float(1.0 / fc.gm1);   // R / (gamma - 1) in the non-dimensional units (R = 1)
     const T eps_r = kMixed ? T(fc.eps_rho) : T(kWenoEps);
     const T eps_m = kMixed ? T(fc.eps_m) : T(kWenoEps);
     const T eps_T = kMixed ? T(fc.eps_T) : T(kWenoEps);
@@ -415,18 +416,30 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
                 T l[5], r[5];
                 if constexpr (kMixed) {
+                    // rho with rho u, and rho v with rho w: two WENO scalars per packed instruction
 #pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const int o = q * kWC + c;
-                        weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], q == 0 ? eps_r : eps_m, l[q], r[q]);
+                    for (int q = 0; q < 4; q += 2) {
+                        const int oa = q * kWC + c, ob = oa + kWC;
+                        F2 lq, rq;
+                        weno_scalar<F2>(F2(s0[oa], s0[ob]), F2(s1[oa], s1[ob]), F2(s2[oa], s2[ob]), F2(s3[oa], s3[ob]),
+                                        F2(s4[oa], s4[ob]), F2(s5[oa], s5[ob]), F2(q == 0 ? eps_r : eps_m, eps_m), lq,
+                                        rq);
+                        l[q] = lq.lo();
+                        l[q + 1] = lq.hi();
+                        r[q] = rq.lo();
+                        r[q + 1] = rq.hi();
                     }
                     T Tl, Tr;
                     {
                         const int o = 5 * kWC + c;
                         weno_scalar<T>(s0[o], s1[o], s2[o], s3[o], s4[o], s5[o], eps_T, Tl, Tr);
                     }
-                    l[4] = face_energy<T>(l[0], l[1], l[2], l[3], Tl, ph);
-                    r[4] = face_energy<T>(r[0], r[1], r[2], r[3], Tr, ph);
+                    // both face energies, src/update.cpp:673-674, one side per lane
+                    const F2 rr(l[0], r[0]), mx(l[1], r[1]), my(l[2], r[2]), mz(l[3], r[3]);
+                    const F2 ke = F2(0.5f) * (mx * mx + my * my + mz * mz) / rr;
+                    const F2 e = F2(rr * F2(Tl, Tr)) * F2(cv_mixed) + ke;
+                    l[4] = e.lo();
+                    r[4] = e.hi();
                 } else {
                     // FP64: the weighted averages of rho, rho u, rho v, rho w share one division among
                     // their eight denominators (each between 20 eps^3 and about IS^3, so the
