@@ -29,7 +29,7 @@ EXPORTS = [
     "gkm_ensemble_member", "gkm_ensemble_step", "gkm_ensemble_step_timed", "gkm_ensemble_autotune",
     "gkm_ensemble_sweep_config", "gkm_ensemble_launch_count", "gkm_ensemble_synchronize", "gkm_ensemble_stream",
     "gkm_particle_props", "gkm_particle_stats_compute", "gkm_write_field", "gkm_write_particles", "gkm_write_time",
-    "gkm_write_reinit", "gkm_set_pipeline", "gkm_ensemble_segments",
+    "gkm_write_reinit", "gkm_set_pipeline", "gkm_ensemble_segments", "gkm_set_sweep_config",
 ]
 
 PROP_COUNT = 41
@@ -109,6 +109,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.gkm_probe_fma_peak.argtypes = [C.c_int32, _dp, _dp]
     L.gkm_autotune.argtypes = [_h, C.c_int32]
     L.gkm_sweep_config.argtypes = [_h, C.POINTER(C.c_int32)]
+    L.gkm_set_sweep_config.argtypes = [_h, C.POINTER(C.c_int32)]
     L.gkm_spline_build_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]
     L.gkm_ensemble_create.argtypes = [C.POINTER(GkmConfig), C.c_int32, C.POINTER(_h)]
     L.gkm_ensemble_destroy.argtypes = [_h]

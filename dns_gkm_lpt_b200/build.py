@@ -21,7 +21,7 @@ OBJDIR = os.path.join(PKG, "lib", "obj")
 LIB = os.path.join(LIBDIR, "libgkm_b200.so")
 
 SOURCES = ["sweep.cu", "sweep_mixed.cu", "lagrangian.cu", "probe.cu", "noalloc.cu", "gkm_capi.cu", "gkm_ensemble.cu", "output.cu"]
-HEADERS = ["gkm_numerics.cuh", "gkm_internal.h", "gkm_handle.h", "sweep_impl.cuh"]
+HEADERS = ["gkm_numerics.cuh", "gkm_internal.h", "gkm_handle.h", "sweep_impl.cuh", "sweep_ws.cuh", "f32x2.cuh"]
 # per-file extra flags: the single-precision sweeps use fast float math
 EXTRA = {"sweep_mixed.cu": ["-use_fast_math", "-DGKM_UNROLL_SIDES=0"]}
 

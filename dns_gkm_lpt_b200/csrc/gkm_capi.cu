@@ -775,6 +775,7 @@ gkm_status gkm_autotune(gkm_handle* h, int32_t reps)
         SweepChoice best = h->sweep[d];
         float best_ms = 1e30f;
         for (int v = 0; v < nvar && st == GKM_OK; v++) {
+            if (!mixed && v == 2 && !gkm::ws_ready()) continue;   // not available on this build
             int last_len = -1;
             for (int ns : nsegs) {
                 SweepChoice c;
@@ -822,6 +823,26 @@ gkm_status gkm_sweep_config(const gkm_handle* h, int32_t out[12])
         out[4 * d + 2] = sh.TA;
         out[4 * d + 3] = h->sweep[d].seg_len;
     }
+    return GKM_OK;
+}
+
+gkm_status gkm_set_sweep_config(gkm_handle* h, const int32_t in[6])
+{
+    if (!h || !in) return GKM_ERR_ARG;
+    const bool mixed = h->cfg.precision == GKM_PREC_MIXED;
+    const int nvar = mixed ? gkm::kSweepVariants32 : gkm::kSweepVariants64;
+    for (int d = 0; d < 3; d++) {
+        const int v = in[2 * d], L = in[2 * d + 1];
+        if (v < 0 || v >= nvar || L < 1) return fail(h, GKM_ERR_ARG, "sweep variant or segment length out of range");
+        if (!mixed && v == 2 && !gkm::ws_ready())
+            return fail(h, GKM_ERR_CONFIG, "the warp-specialized sweep is not available on this build");
+    }
+    for (int d = 0; d < 3; d++) {
+        h->sweep[d].variant = in[2 * d];
+        h->sweep[d].seg_len = in[2 * d + 1] < h->fc.n ? in[2 * d + 1] : h->fc.n;
+        h->sweep[d].nseg = (h->fc.n + h->sweep[d].seg_len - 1) / h->sweep[d].seg_len;
+    }
+    destroy_graphs(h);
     return GKM_OK;
 }
 

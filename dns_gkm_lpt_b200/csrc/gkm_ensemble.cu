@@ -415,7 +415,8 @@ gkm_status gkm_ensemble_autotune(gkm_ensemble* E, int32_t reps)
         return v;
     };
     const std::vector<int> lens = lens_upto(sizes[0]);
-    const int nvar = E->mixed ? gkm::kSweepVariants32 : gkm::kSweepVariants64;
+    // the persistent kernel has the plain window variants only (variant 2 is single-cube)
+    const int nvar = E->mixed ? gkm::kSweepVariants32 : 2;
     const int p = E->mem[0]->parity;
     cudaEvent_t e0, e1;
     ECK(E, cudaEventCreate(&e0));

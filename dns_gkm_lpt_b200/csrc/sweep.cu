@@ -15,6 +15,7 @@
 // wraps A's ghosts and the caller swaps W and A.  The additions run in the
 // reference's left-to-right order with rounding-explicit intrinsics.
 #include "sweep_impl.cuh"
+#include "sweep_ws.cuh"
 
 namespace gkm {
 namespace {
@@ -136,6 +137,29 @@ __global__ void weno_faces_kernel(const double* __restrict__ s, long long n, Phy
     }
 }
 
+// the warp-specialized sweep may run only where its kernels were compiled to the register count
+// its warpgroups' setmaxnreg split draws on (a smaller launch count would leave them waiting)
+bool g_ws_ready = false;
+
+template <int DIR>
+cudaError_t ws_check(bool& ok)
+{
+    cudaFuncAttributes at;
+    cudaError_t e = cudaFuncGetAttributes(&at, sweep_ws_kernel<DIR, SweepTile64b>);
+    if (e != cudaSuccess) return e;
+    ok = ok && at.numRegs == 168;
+    return cudaFuncSetAttribute(sweep_ws_kernel<DIR, SweepTile64b>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sweep_ws_detail::ws_smem_bytes<SweepTile64b>());
+}
+
+template <int DIR>
+cudaError_t launch_ws(SweepArgs a, dim3 grid, cudaStream_t s)
+{
+    sweep_ws_kernel<DIR, SweepTile64b>
+        <<<grid, sweep_ws_detail::kThreads, sweep_ws_detail::ws_smem_bytes<SweepTile64b>(), s>>>(a);
+    return cudaGetLastError();
+}
+
 template <int DIR, class Tile>
 cudaError_t launch_one(const SweepArgs& a, int nseg, cudaStream_t s)
 {
@@ -188,14 +212,22 @@ cudaError_t sweep_prepare()
     if (e == cudaSuccess) e = set_smem<SweepTile64b>();
     if (e == cudaSuccess) e = set_ensemble_smem<double, SweepTile64a>();
     if (e == cudaSuccess) e = set_ensemble_smem<double, SweepTile64b>();
+    bool ok = true;
+    if (e == cudaSuccess) e = ws_check<0>(ok);
+    if (e == cudaSuccess) e = ws_check<1>(ok);
+    if (e == cudaSuccess) e = ws_check<2>(ok);
+    g_ws_ready = e == cudaSuccess && ok;
     return e;
 }
+
+bool ws_ready() { return g_ws_ready; }
 
 cudaError_t launch_ensemble_sweep64(int dir, int variant, const MemberDev* mem, const long long* off,
                                     const long long* order, int nm, int parity, unsigned long long* next,
                                     cudaStream_t s)
 {
-    if (variant == 1)
+    // the ensemble's persistent kernel has no warp-specialized form: variant 2 runs as variant 1
+    if (variant >= 1)
         return launch_ensemble_sweep_t<double, SweepTile64b>(dir, mem, off, order, nm, parity, next, s);
     return launch_ensemble_sweep_t<double, SweepTile64a>(dir, mem, off, order, nm, parity, next, s);
 }
@@ -213,13 +245,20 @@ cudaError_t launch_ensemble_halo(const MemberDev* mem, const long long* off, int
 SweepShape sweep_shape(bool mixed, int variant)
 {
     if (mixed) return {0, SweepTile32a::TB, SweepTile32a::TA, SweepTile32a::ctas};
+    if (variant == 2) return {2, SweepTile64b::TB, SweepTile64b::TA, 1};
     if (variant == 1) return {1, SweepTile64b::TB, SweepTile64b::TA, SweepTile64b::ctas};
     return {0, SweepTile64a::TB, SweepTile64a::TA, SweepTile64a::ctas};
 }
 
 cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s)
 {
-    if (variant == 1) {
+    if (variant == 2 && g_ws_ready) {
+        const dim3 grid((a.fc.n + 15) / 16, (a.fc.n + 15) / 16, nseg);
+        if (dir == 0) return launch_ws<0>(a, grid, s);
+        if (dir == 1) return launch_ws<1>(a, grid, s);
+        return launch_ws<2>(a, grid, s);
+    }
+    if (variant >= 1) {
         if (dir == 0) return launch_one<0, SweepTile64b>(a, nseg, s);
         if (dir == 1) return launch_one<1, SweepTile64b>(a, nseg, s);
         return launch_one<2, SweepTile64b>(a, nseg, s);
@@ -231,7 +270,8 @@ cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cud
 
 cudaError_t launch_sweep_rows(int dir, int variant, SweepArgs a, int j0, int j1, cudaStream_t s)
 {
-    if (variant == 1) return launch_sweep_rows_t<double, SweepTile64b>(dir, a, j0, j1, s);
+    // the pipelined plug point runs the plain kernels (variant 2 as variant 1)
+    if (variant >= 1) return launch_sweep_rows_t<double, SweepTile64b>(dir, a, j0, j1, s);
     return launch_sweep_rows_t<double, SweepTile64a>(dir, a, j0, j1, s);
 }
 

@@ -176,6 +176,11 @@ class Solver:
         return [{"dir": "xyz"[d], "variant": out[4 * d], "window": [out[4 * d + 1], out[4 * d + 2]],
                  "segment": out[4 * d + 3]} for d in range(3)]
 
+    def set_sweep_config(self, shapes) -> None:
+        """shapes: three (window variant, segment length) pairs for x, y, z."""
+        arr = (C.c_int32 * 6)(*[int(x) for pair in shapes for x in pair])
+        self._check(self.L.gkm_set_sweep_config(self.h, arr))
+
     def launch_count(self) -> int:
         n = C.c_int64()
         self._check(self.L.gkm_launch_count(self.h, C.byref(n)))

@@ -189,8 +189,16 @@ gkm_status gkm_step_timed(gkm_handle* h, int32_t nsteps, int32_t with_particles,
  * keeps the fastest.  The state is not changed; captured graphs are rebuilt. */
 gkm_status gkm_autotune(gkm_handle* h, int32_t reps);
 /* The sweep shapes in use: for x, y, z in turn: window variant, window width,
- * window height, segment length (faces per CTA along the normal). */
+ * window height, segment length (faces per CTA along the normal).  FP64 window
+ * variants: 0 = 16 x 8 (two CTAs per SM), 1 = 16 x 16, 2 = 16 x 16
+ * warp-specialized (a producer warpgroup reconstructs the next face plane while
+ * two consumer warpgroups compute fluxes; single cubes; the plug-point pipeline
+ * of gkm_evolve runs it as variant 1).  FP32: 0 = 16 x 8. */
 gkm_status gkm_sweep_config(const gkm_handle* h, int32_t out[12]);
+/* Set the sweep shapes (no reference counterpart): for x, y, z in turn the
+ * window variant and the segment length (in[2d], in[2d+1]).  GKM_ERR_CONFIG for
+ * a variant this precision or this GPU does not have. */
+gkm_status gkm_set_sweep_config(gkm_handle* h, const int32_t in[6]);
 
 /* Kernels this handle has launched so far (graph replays count their kernels). */
 gkm_status gkm_launch_count(const gkm_handle* h, int64_t* count);

@@ -284,3 +284,30 @@ def test_autotune_keeps_state_and_results(prec):
         plain = s.download_state()
     # every face sees the same inputs whatever the window or segment, so the results agree
     assert rel_l2(tuned, plain).max() <= 1e-13
+
+
+def test_warp_specialized_sweep_matches_reference_and_plain_sweep(golden):
+    """Window variant 2 (a producer warpgroup reconstructs the next face plane while two consumer
+    warpgroups compute fluxes) against the reference CPU build's 16^3 fields (1e-12) and against
+    the plain 16 x 16 sweep (variant 1) at 48^3 (1e-14: the same arithmetic, rounded differently
+    only where the plain sweep splits a window's last cells into single WENO scalars)."""
+    g = golden["field_16"]
+    P, W0 = w0_of(g)
+    pos0 = ic.particles_to_reference_order(g["particles_xyz"])
+    with Solver(P, cfl=float(g["cfl"]), max_particles=len(pos0)) as s:
+        s.set_sweep_config([(2, 8), (2, 16), (2, 5)])
+        assert [c["variant"] for c in s.sweep_config()] == [2, 2, 2]
+        s.upload_state(W0)
+        s.particles_upload(pos0)
+        s.step(len(g["dt"]))
+        assert rel_l2(s.download_state(), g["W_final"]).max() <= FIELD_TOL
+    P, W0 = case(48, 0.4, 50.0, 5)
+    out = {}
+    for var in (1, 2):
+        with Solver(P, cfl=0.5) as s:
+            s.set_sweep_config([(var, 24)] * 3)
+            s.upload_state(W0)
+            s.evolve_eulerian(4)
+            out[var] = s.download_state()
+            s.clock()
+    assert rel_l2(out[2], out[1]).max() <= 1e-14
