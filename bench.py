@@ -465,7 +465,13 @@ def ours(args, rank: int, world: int, local_rank: int):
     s.set_stream(stream.cuda_stream)
     s.upload_state(W0)
     s.particles_upload(pos0)
-    sweep_cfg = s.autotune(args.autotune_reps) if args.autotune_reps > 0 else s.sweep_config()
+    if args.shapes:
+        # fixed sweep shapes, e.g. "x=2:64,y=2:64,z=1:64" (window variant : segment length per direction)
+        shapes = dict(item.split("=") for item in args.shapes.split(","))
+        s.set_sweep_config([tuple(int(v) for v in shapes[d].split(":")) for d in "xyz"])
+        sweep_cfg = s.sweep_config()
+    else:
+        sweep_cfg = s.autotune(args.autotune_reps) if args.autotune_reps > 0 else s.sweep_config()
     s.step_timed(args.warmup, True)
     torch.cuda.synchronize()
 
@@ -648,6 +654,9 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="form of the main line")
     ap.add_argument("--spline-precision", default="fp64", choices=["fp64", "fp32"],
                     help="velocity-spline coefficients of the main line (fp32: same FP64 solves, stored rounded)")
+    ap.add_argument("--shapes", default="",
+                    help="fixed sweep shapes of the main line instead of the autotuner's, e.g. x=2:64,y=2:64,z=1:64 "
+                         "(window variant:segment length)")
     ap.add_argument("--autotune-reps", type=int, default=2,
                     help="timed launches per sweep shape; 0 keeps the default shapes (profiling runs)")
     args = ap.parse_args()
