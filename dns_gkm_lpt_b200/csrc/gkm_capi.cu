@@ -95,19 +95,31 @@ void destroy_graphs(gkm_handle* h)
         }
 }
 
-// tensor map of the state buffer W for sweep direction dir and window variant (FP64 x, y)
+// tensor maps (FP64), 4 per buffer and window variant: x slab, y slab, z accumulator brick, z slab
+// box.  sweep_tmap: the map of buffer W for the slab copies of direction dir; sweep_tmap_acc: the
+// map of buffer A for the z sweep's accumulator bricks
+const void* tmap_at(const gkm_handle* h, const double* buf, int variant, int kind)
+{
+    if (!h->d_tmaps || h->cfg.precision == GKM_PREC_MIXED) return nullptr;
+    const int b = (buf == h->buf[0]) ? 0 : (buf == h->buf[1] ? 1 : -1);
+    if (b < 0) return nullptr;
+    return h->d_tmaps + sizeof(CUtensorMap) * (size_t)((b * gkm::kSweepVariants64 + variant) * 4 + kind);
+}
 const void* sweep_tmap(const gkm_handle* h, const double* W, int dir, int variant)
 {
-    if (!h->d_tmaps || dir > 1 || h->cfg.precision == GKM_PREC_MIXED) return nullptr;
-    const int b = (W == h->buf[0]) ? 0 : (W == h->buf[1] ? 1 : -1);
-    if (b < 0) return nullptr;
-    return h->d_tmaps + sizeof(CUtensorMap) * (size_t)((b * gkm::kSweepVariants64 + variant) * 2 + dir);
+    return tmap_at(h, W, variant, dir == 2 ? 3 : dir);
+}
+const void* sweep_tmap_acc(const gkm_handle* h, const double* A, int dir, int variant)
+{
+    return dir == 2 ? tmap_at(h, A, variant, 2) : nullptr;
 }
 
-// Encode the tensor maps: W as a 4-D tensor (k, i, j, q) of doubles, dims (nt, nt, nt, 5); box
-// (WB, 1, WA, 5) for the x sweep (window j x k at one i) and (WB, WA, 1, 5) for the y sweep
-// (window i x k at one j).  The row strides must be multiples of 16 bytes, so nt must be even;
-// otherwise (or without the driver entry point) the sweeps copy slabs with cp.async.
+// Encode the tensor maps: each buffer as a 4-D tensor (k, i, j, q) of doubles, dims (nt, nt, nt, 5);
+// boxes (WB, 1, WA, 5) for the x sweep's slabs (window j x k at one i), (WB, WA, 1, 5) for the y
+// sweep's (window i x k at one j), (2, TB, TA, 5) for the z sweep's accumulator bricks (two k-cells
+// of the window i x j) and (2, WB, WA, 5) for its slabs (two k-planes of the window and its halo).
+// The row strides must be multiples of 16 bytes, so nt must be even; otherwise (or without the
+// driver entry point) the sweeps move every value with cp.async and plain loads and stores.
 cudaError_t setup_tensor_maps(gkm_handle* h)
 {
     if (h->cfg.precision == GKM_PREC_MIXED || h->fc.nt % 2) return cudaSuccess;
@@ -126,15 +138,17 @@ cudaError_t setup_tensor_maps(gkm_handle* h)
     const cuuint64_t dims[4] = {nt, nt, nt, 5};
     const cuuint64_t strides[3] = {nt * 8, nt * nt * 8, nt * nt * nt * 8};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    const int nmaps = 2 * gkm::kSweepVariants64 * 2;
+    const int nmaps = 2 * gkm::kSweepVariants64 * 4;
     std::vector<CUtensorMap> maps((size_t)nmaps);
     for (int b = 0; b < 2; b++)
         for (int v = 0; v < gkm::kSweepVariants64; v++)
-            for (int d = 0; d < 2; d++) {
+            for (int d = 0; d < 4; d++) {
                 const gkm::SweepShape sh = gkm::sweep_shape(false, v);
                 const cuuint32_t WB = (cuuint32_t)sh.TB + 2, WA = (cuuint32_t)sh.TA + 2;
-                const cuuint32_t box[4] = {WB, d == 0 ? 1u : WA, d == 0 ? WA : 1u, 5};
-                CUresult r = encode(&maps[(size_t)((b * gkm::kSweepVariants64 + v) * 2 + d)],
+                const cuuint32_t boxes[4][4] = {
+                    {WB, 1u, WA, 5}, {WB, WA, 1u, 5}, {2u, (cuuint32_t)sh.TB, (cuuint32_t)sh.TA, 5}, {2u, WB, WA, 5}};
+                const cuuint32_t* box = boxes[d];
+                CUresult r = encode(&maps[(size_t)((b * gkm::kSweepVariants64 + v) * 4 + d)],
                                     CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, h->buf[b], dims, strides, box, estr,
                                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -151,6 +165,7 @@ cudaError_t launch_sweep_any(gkm_handle* h, int dir, gkm::SweepArgs a)
     const SweepChoice& c = h->sweep[dir];
     a.seg_len = c.seg_len;
     a.tmap = sweep_tmap(h, a.W, dir, c.variant);
+    a.tmap_acc = sweep_tmap_acc(h, a.A, dir, c.variant);
     a.wait_probe = h->cfg.test_wait_probe;
     if (h->cfg.precision == GKM_PREC_MIXED) return gkm::launch_sweep_mixed(dir, c.variant, a, c.nseg, h->stream);
     return gkm::launch_sweep(dir, c.variant, a, c.nseg, h->stream);
@@ -1011,6 +1026,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
             ad.seg_len = (d == 1) ? j1 - j0 : std::min(h->sweep[d].seg_len, C);
             const int v = h->sweep[d].variant;
             ad.tmap = sweep_tmap(h, ad.W, d, v);
+            ad.tmap_acc = sweep_tmap_acc(h, ad.A, d, v);
             CK(h, mixed ? gkm::launch_sweep_mixed_rows(d, v, ad, j0, j1, s) : gkm::launch_sweep_rows(d, v, ad, j0, j1, s));
         }
         CK(h, gkm::launch_halo_planes(A, fc, 3 + j0, 3 + j1, s));

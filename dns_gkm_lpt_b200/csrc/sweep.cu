@@ -165,20 +165,22 @@ cudaError_t launch_one(const SweepArgs& a, int nseg, cudaStream_t s)
 {
     dim3 grid((a.fc.n + Tile::TB - 1) / Tile::TB, (a.fc.n + Tile::TA - 1) / Tile::TA, nseg);
     dim3 block(Tile::TB, Tile::TA);
-    sweep_kernel<DIR, double, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<double, Tile>(), s>>>(a);
+    sweep_kernel<DIR, double, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<double, Tile, DIR>(), s>>>(a);
     return cudaGetLastError();
 }
 
 template <class Tile>
 cudaError_t set_smem()
 {
-    const int bytes = (int)sweep_detail::sweep_smem_bytes<double, Tile>();
-    cudaError_t e =
-        cudaFuncSetAttribute(sweep_kernel<0, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    using sweep_detail::sweep_smem_bytes;
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<0, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sweep_smem_bytes<double, Tile, 0>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<1, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(sweep_kernel<1, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sweep_smem_bytes<double, Tile, 1>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<2, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(sweep_kernel<2, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sweep_smem_bytes<double, Tile, 2>());
     return e;
 }
 

@@ -156,10 +156,36 @@ __host__ __device__ constexpr bool sweep_lean()
     return sizeof(T) == 4 && DIR != 1;
 }
 
+// FP64 z sweep: the accumulator of two consecutive k-cells of the window moves as one brick, a
+// box (2, TB, TA, 5) of the (k, i, j, q) tensor, loaded and stored by bulk tensor copies; two
+// bricks in flight.  The staging area of the other sweeps shares their space.  The slabs arrive the
+// same way, two planes of the window and its halo (a box (2, WB, WA, 5)) in a landing area.
+template <class Tile>
+__host__ __device__ constexpr int zbrick_elems()
+{
+    return 5 * Tile::TA * Tile::TB * 2;
+}
+template <class Tile>
+__host__ __device__ constexpr int zland_elems()
+{
+    return 5 * Tile::WC * 2;
+}
+
+template <class T, int DIR>
+__host__ __device__ constexpr bool sweep_zpairs()
+{
+    return DIR == 2 && sizeof(T) == 8;
+}
+
 template <class T, class Tile, int DIR = 1>
 __host__ __device__ constexpr size_t sweep_smem_bytes()
 {
     if (sweep_lean<T, DIR>()) return sizeof(T) * (size_t)(kRing * slot_elems<T, Tile>() + 10 * Tile::WC);
+    // ring + reconstructions, 128 bytes of slack to align the bricks, two accumulator bricks, the
+    // slab landing area, three mbarriers
+    if (sweep_zpairs<T, DIR>())
+        return (sweep_ring_bytes<T, Tile>() + 128 + sizeof(double) * (2 * zbrick_elems<Tile>() + zland_elems<Tile>()) + 24 +
+                15) / 16 * 16;
     return sweep_ring_bytes<T, Tile>() + sizeof(double) * 5 * (size_t)Tile::threads + 16;   // + mbarrier
 }
 
@@ -206,6 +232,20 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity,
     return false;
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// shared -> global bulk tensor copy of a box whose origin (c0, c1, c2, 0) is inside the tensor
+// (elements beyond its extent are not written), and the waits on such copies: until each has read
+// its shared-memory source, and until each has completed
+__device__ __forceinline__ void tma_box_store(const void* tmap, int c0, int c1, int c2, unsigned src)
+{
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];\n" ::"l"(tmap),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(0), "r"(src)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// generic-proxy shared-memory writes of this thread, ordered before later bulk copies that read them
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 // retire `bytes` of a barrier phase's expected transaction count without a copy (the failure-detection
 // test hook takes back the bytes it added beyond what its copy delivers)
 __device__ __forceinline__ void mbar_complete_tx(unsigned bar, unsigned bytes)
@@ -274,8 +314,18 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     T* ring = sweep_lean<T, DIR>() ? reinterpret_cast<T*>(smem_raw)
                                    : reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     T* rec = ring + kRing * kSlot;
-    double* stage = reinterpret_cast<double*>(smem_raw + sweep_ring_bytes<T, Tile>());   // [5][threads]
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(stage + 5 * kSweepThreads);
+    constexpr bool kZPairs = sweep_zpairs<T, DIR>();
+    constexpr int kZB = zbrick_elems<Tile>();
+    // FP64 z sweep: two accumulator bricks (128-byte aligned for the bulk copies), whose space also
+    // serves as the staging area, the slab landing area [q][a][b][2], then three mbarriers (the two
+    // bricks', the landing area's)
+    double* stage =
+        kZPairs ? reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw + sweep_ring_bytes<T, Tile>()) + 127) &
+                                            ~uintptr_t(127))
+                : reinterpret_cast<double*>(smem_raw + sweep_ring_bytes<T, Tile>());   // [5][threads]
+    double* land = stage + 2 * kZB;
+    unsigned long long* bar =
+        reinterpret_cast<unsigned long long*>(kZPairs ? land + zland_elems<Tile>() : stage + 5 * kSweepThreads);
     const FieldConst& fc = a.fc;
     const int n = fc.n, nt = fc.nt;
     const long long nt3 = fc.nt3;
@@ -374,6 +424,68 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
 
     for (int f = f_begin - 3; f < f_begin + 2; f++) load_slab(f);
 
+    // FP64 z sweep.  Its normal k is the contiguous axis, so one value per window cell and plane is
+    // 8 bytes of a different 128-byte line; the window's 1,620 lines per plane (16 x 16 windows)
+    // do not stay in L1 for the four planes a 32-byte sector holds, and per-element loads fetch
+    // each sector from L2 four times.  Planes k, k+1 with k + 3 even travel together instead.
+    // Slabs (a.tmap): the two planes of the window and its halo land as one box in the landing area
+    // and each thread moves its cells' values into the plane's ring slot as it forms their
+    // temperature; the next box is requested once the landing area's second plane is in the ring,
+    // one face before it is needed.  Accumulator (a.tmap_acc): cells k, k+1 form a pair, and the
+    // pairs whose two cells both lie in this segment move as bricks: each brick is loaded while the
+    // faces before it are computed (the load of a pair issued when the previous pair's second cell
+    // starts), updated in shared memory by its two cells and stored once the second cell is
+    // written.  A cell whose partner lies in another segment (at most the first and the last of
+    // each) is read and written directly, so no two CTAs store the same brick.
+    const bool zslab = kZPairs && a.tmap != nullptr;
+    const bool zpair = kZPairs && a.tmap_acc != nullptr;
+    const unsigned zbar = smem_u32(bar), lbar = zbar + 16u;
+    unsigned zph = 0;   // bit b: the phase of brick buffer b's barrier awaited next
+    unsigned lph = 0;   // the phase of the landing area's barrier awaited next
+    auto first_of_pair = [](int f) { return ((f + 3) & 1) == 0; };
+    auto paired = [&](int f) {
+        const int p = first_of_pair(f) ? f + 1 : f - 1;
+        return p >= f_begin && p < f_end;
+    };
+    auto zbuf = [](int f) { return ((f + 3) >> 1) & 1; };
+    auto zload = [&](int pf) {   // the brick of the pair whose first cell is pf (one thread)
+        const int b = zbuf(pf);
+        tma_slab_load(smem_u32(stage + b * kZB), a.tmap_acc, pf + 3, b0 + 3, a0 + 3, (unsigned)(kZB * sizeof(double)),
+                      zbar + 8u * b);
+    };
+    auto zslab_load = [&](int p) {   // planes p, p+1 (p + 3 even) of the window and its halo (one thread)
+        tma_slab_load(smem_u32(land), a.tmap, p + 3, b0 + 2, a0 + 2, (unsigned)(zland_elems<Tile>() * sizeof(double)), lbar);
+    };
+    // plane f from the landing area into its ring slot, with its temperature
+    auto finish_slab_landed = [&](int f) {
+        T* s = slot(f);
+        const double* L = land + ((f + 3) & 1);
+        for (int c = tid; c < kWC; c += kSweepThreads) {
+            const int aa = c / kWB, bb = c - aa * kWB;
+            if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
+            const double r = L[2 * c], m1 = L[2 * (kWC + c)], m2 = L[2 * (2 * kWC + c)], m3 = L[2 * (3 * kWC + c)],
+                         E = L[2 * (4 * kWC + c)];
+            s[c] = r;
+            s[kWC + c] = m1;
+            s[2 * kWC + c] = m2;
+            s[3 * kWC + c] = m3;
+            s[4 * kWC + c] = E;
+            s[5 * kWC + c] = temperature<T>(r, m1, m2, m3, E, ph);
+        }
+    };
+    if (zpair || zslab) {
+        if (tid == 0) {
+            mbar_init(zbar);
+            mbar_init(zbar + 8u);
+            mbar_init(lbar);
+        }
+        __syncthreads();
+        const int pf0 = first_of_pair(f_begin) ? f_begin : f_begin + 1;
+        if (tid == 0 && zpair && pf0 + 1 < f_end) zload(pf0);
+        // the first plane not loaded directly, f_begin + 3, and its partner
+        if (tid == 0 && zslab) zslab_load(first_of_pair(f_begin + 3) ? f_begin + 3 : f_begin + 2);
+    }
+
     const bool active = (a0 + ty < n) && (b0 + tx < n);
     const int cc = (ty + 1) * kWB + (tx + 1);
     const long long cell0 = (a0 + ty + 3) * st.sA + (b0 + tx + 3) * st.sB;
@@ -392,12 +504,31 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 }
                 if (!mbar_wait_bounded(bar_u32, tma_phase)) atomicOr(&a.clock->status, 2);
                 tma_phase ^= 1u;
+            } else if (zslab) {
+                // a box holds planes f+3 and f+4, or f+2 and f+3: wait for it where its first plane is taken
+                if (first_of_pair(f + 3) || f == f_begin) {
+                    if (!mbar_wait_bounded(lbar, lph)) atomicOr(&a.clock->status, 2);
+                    lph ^= 1u;
+                }
             } else {
                 cp_async_wait_all();
             }
-            finish_slab(f + 3);
+            if (zslab) finish_slab_landed(f + 3);
+            else finish_slab(f + 3);
         }
         __syncthreads();
+        // the landing area's second plane is in the ring: the next two planes, wanted from the next face on
+        if (zslab && tid == 0 && f >= f_begin && !first_of_pair(f + 3) && f + 1 < f_end) zslab_load(f + 4);
+        if (zpair && tid == 0 && f > f_begin) {
+            // the pair the previous cell completed goes out (its writes were fenced before the barrier)
+            if (!first_of_pair(f - 1) && paired(f - 1))
+                tma_box_store(a.tmap_acc, f + 1, b0 + 3, a0 + 3, smem_u32(stage + zbuf(f - 1) * kZB));
+            // the next pair comes in, into the buffer whose store left one cell ago
+            if (!first_of_pair(f) && paired(f) && f + 2 < f_end) {
+                bulk_wait_read();
+                zload(f + 1);
+            }
+        }
         // reconstruct every face of the window once (the reference repeats this 5x per face)
         {
             const T* s0 = slot(f - 2);
@@ -516,7 +647,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                                       ((probe && f == f_begin - 1) ? kProbeExtraBytes : 0u),
                                   bar_u32);
                 }
-            } else {
+            } else if (!zslab) {
                 issue_slab(f + 4);
             }
         }
@@ -558,7 +689,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             // is computed (the mixed z sweep, which also re-reads the state, loads it directly:
             // measured faster there)
             constexpr bool kFetchA = DIR == 1 || (DIR == 2 && !kMixed);
-            const bool fetch_a = kFetchA && f >= f_begin;
+            const bool fetch_a = kFetchA && f >= f_begin && !zpair;
             if (fetch_a) {
 #pragma unroll
                 for (int q = 0; q < 5; q++) cp_async8(&stage[q * kSweepThreads + tid], &a.A[q * nt3 + ci]);
@@ -585,15 +716,24 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                     }
                 } else {
                     double wn[5];
+                    const bool zp = zpair && paired(f);
+                    // the cell's accumulator in its pair's brick, laid out [q][a][b][k & 1]
+                    double* zc = stage + zbuf(f) * kZB + (ty * kTB + tx) * 2 + ((f + 3) & 1);
+                    if (zp && first_of_pair(f)) {
+                        if (!mbar_wait_bounded(zbar + 8u * zbuf(f), (zph >> zbuf(f)) & 1u)) atomicOr(&a.clock->status, 2);
+                    }
 #pragma unroll
                     for (int q = 0; q < 5; q++) {
-                        double acc = kFetchA ? stage[q * kSweepThreads + tid] : a.A[q * nt3 + ci];
+                        double acc = zp ? zc[q * 2 * kTA * kTB]
+                                        : ((kFetchA && !zpair) ? stage[q * kSweepThreads + tid] : a.A[q * nt3 + ci]);
                         double s = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
                         // the cell's FP64 state (the FP64 ring holds it; the mixed ring has FP32 copies)
                         const double wq = kMixed ? W[q * nt3 + ci] : (double)wl[q * kWC + cc];
                         wn[q] = __dsub_rn(wq, __dmul_rn(fc.inv_dx, s));
-                        a.A[q * nt3 + ci] = wn[q];
+                        if (zp) zc[q * 2 * kTA * kTB] = wn[q];
+                        else a.A[q * nt3 + ci] = wn[q];
                     }
+                    if (zp && !first_of_pair(f)) fence_async_shared();   // the brick's copy out reads it
                     const double ws = wave_speed_recip(wn, fc.gam, fc.gm1);
                     if (!isfinite(ws) || !(wn[0] > 0.0)) bad = true;
                     else wmax = ws > wmax ? ws : wmax;
@@ -601,6 +741,19 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             }
 #pragma unroll
             for (int q = 0; q < 5; q++) Fprev[q] = F[q];
+        }
+        if (zpair && f >= f_begin && first_of_pair(f) && paired(f)) zph ^= 1u << zbuf(f);
+    }
+    if (zpair || zslab) {
+        __syncthreads();   // the last pair's writes, fenced, before its copy out
+        if (tid == 0) {
+            const int fl = f_end - 1;
+            if (zpair && !first_of_pair(fl) && paired(fl))
+                tma_box_store(a.tmap_acc, fl + 2, b0 + 3, a0 + 3, smem_u32(stage + zbuf(fl) * kZB));
+            bulk_wait_all();   // every brick stored before the shared memory is reused or released
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(zbar) : "memory");
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(zbar + 8u) : "memory");
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(lbar) : "memory");
         }
     }
     if (DIR == 2) {
@@ -650,11 +803,13 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
         const int bz = (int)(local % nseg);
         const long long t = local / nseg;
         SweepArgs a;
-        // FP64 x / y sweeps: the member's tensor map of the buffer read (variant 1 = 16x16 windows)
+        // FP64: the member's tensor maps (4 per buffer and window variant: x slab, y slab, z
+        // accumulator brick, z slab box) of the buffer read and, for the z sweep, the buffer written;
+        // variant 1 = 16x16 windows
         constexpr int kVariant = (sizeof(T) == 8 && Tile::TA == 16) ? 1 : 0;
-        a.tmap = (sizeof(T) == 8 && DIR < 2 && md.tmaps)
-                     ? md.tmaps + 128 * ((parity * kSweepVariants64 + kVariant) * 2 + DIR)
-                     : nullptr;
+        const bool maps = sizeof(T) == 8 && md.tmaps;
+        a.tmap = maps ? md.tmaps + 128 * ((parity * kSweepVariants64 + kVariant) * 4 + (DIR == 2 ? 3 : DIR)) : nullptr;
+        a.tmap_acc = (maps && DIR == 2) ? md.tmaps + 128 * (((parity ^ 1) * kSweepVariants64 + kVariant) * 4 + 2) : nullptr;
         a.tile_a0 = 0;
         a.f0 = 0;
         a.f1 = 0;
@@ -721,13 +876,15 @@ cudaError_t launch_ensemble_sweep_t(int dir, const MemberDev* mem, const long lo
 template <class T, class Tile>
 cudaError_t set_ensemble_smem()
 {
-    const int bytes = (int)sweep_detail::sweep_smem_bytes<T, Tile>();
+    using sweep_detail::sweep_smem_bytes;
     cudaError_t e = cudaFuncSetAttribute(ensemble_sweep_kernel<0, T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         bytes);
+                                         (int)sweep_smem_bytes<T, Tile, 0>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(ensemble_sweep_kernel<1, T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(ensemble_sweep_kernel<1, T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sweep_smem_bytes<T, Tile, 1>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(ensemble_sweep_kernel<2, T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(ensemble_sweep_kernel<2, T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sweep_smem_bytes<T, Tile, 2>());
     return e;
 }
 
