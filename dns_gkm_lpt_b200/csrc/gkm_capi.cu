@@ -95,12 +95,13 @@ void destroy_graphs(gkm_handle* h)
         }
 }
 
-// tensor maps (FP64), 4 per buffer and window variant: x slab, y slab, z accumulator brick, z slab
-// box.  sweep_tmap: the map of buffer W for the slab copies of direction dir; sweep_tmap_acc: the
-// map of buffer A for the z sweep's accumulator bricks
+// tensor maps, 4 per buffer and window variant: x slab, y slab, z brick, z slab box (the mixed
+// form has the maps of its one window).  sweep_tmap: the map of buffer W for the slab copies of
+// direction dir; sweep_tmap_acc: the map of buffer A for the z sweep's accumulator bricks;
+// sweep_tmap_wb: the map of buffer W for the mixed z sweep's FP64 state bricks
 const void* tmap_at(const gkm_handle* h, const double* buf, int variant, int kind)
 {
-    if (!h->d_tmaps || h->cfg.precision == GKM_PREC_MIXED) return nullptr;
+    if (!h->d_tmaps) return nullptr;
     const int b = (buf == h->buf[0]) ? 0 : (buf == h->buf[1] ? 1 : -1);
     if (b < 0) return nullptr;
     return h->d_tmaps + sizeof(CUtensorMap) * (size_t)((b * gkm::kSweepVariants64 + variant) * 4 + kind);
@@ -113,6 +114,10 @@ const void* sweep_tmap_acc(const gkm_handle* h, const double* A, int dir, int va
 {
     return dir == 2 ? tmap_at(h, A, variant, 2) : nullptr;
 }
+const void* sweep_tmap_wb(const gkm_handle* h, const double* W, int dir, int variant)
+{
+    return (dir == 2 && h->cfg.precision == GKM_PREC_MIXED) ? tmap_at(h, W, variant, 2) : nullptr;
+}
 
 // Encode the tensor maps: each buffer as a 4-D tensor (k, i, j, q) of doubles, dims (nt, nt, nt, 5);
 // boxes (WB, 1, WA, 5) for the x sweep's slabs (window j x k at one i), (WB, WA, 1, 5) for the y
@@ -122,7 +127,8 @@ const void* sweep_tmap_acc(const gkm_handle* h, const double* A, int dir, int va
 // driver entry point) the sweeps move every value with cp.async and plain loads and stores.
 cudaError_t setup_tensor_maps(gkm_handle* h)
 {
-    if (h->cfg.precision == GKM_PREC_MIXED || h->fc.nt % 2) return cudaSuccess;
+    if (h->fc.nt % 2) return cudaSuccess;
+    const bool mixed = h->cfg.precision == GKM_PREC_MIXED;
     using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -141,9 +147,9 @@ cudaError_t setup_tensor_maps(gkm_handle* h)
     const int nmaps = 2 * gkm::kSweepVariants64 * 4;
     std::vector<CUtensorMap> maps((size_t)nmaps);
     for (int b = 0; b < 2; b++)
-        for (int v = 0; v < gkm::kSweepVariants64; v++)
+        for (int v = 0; v < (mixed ? gkm::kSweepVariants32 : gkm::kSweepVariants64); v++)
             for (int d = 0; d < 4; d++) {
-                const gkm::SweepShape sh = gkm::sweep_shape(false, v);
+                const gkm::SweepShape sh = gkm::sweep_shape(mixed, v);
                 const cuuint32_t WB = (cuuint32_t)sh.TB + 2, WA = (cuuint32_t)sh.TA + 2;
                 const cuuint32_t boxes[4][4] = {
                     {WB, 1u, WA, 5}, {WB, WA, 1u, 5}, {2u, (cuuint32_t)sh.TB, (cuuint32_t)sh.TA, 5}, {2u, WB, WA, 5}};
@@ -166,6 +172,7 @@ cudaError_t launch_sweep_any(gkm_handle* h, int dir, gkm::SweepArgs a)
     a.seg_len = c.seg_len;
     a.tmap = sweep_tmap(h, a.W, dir, c.variant);
     a.tmap_acc = sweep_tmap_acc(h, a.A, dir, c.variant);
+    a.tmap_wb = sweep_tmap_wb(h, a.W, dir, c.variant);
     a.wait_probe = h->cfg.test_wait_probe;
     if (h->cfg.precision == GKM_PREC_MIXED) return gkm::launch_sweep_mixed(dir, c.variant, a, c.nseg, h->stream);
     return gkm::launch_sweep(dir, c.variant, a, c.nseg, h->stream);
@@ -1027,6 +1034,7 @@ gkm_status evolve_pipelined(gkm_handle* h, double* const W[5], double dt)
             const int v = h->sweep[d].variant;
             ad.tmap = sweep_tmap(h, ad.W, d, v);
             ad.tmap_acc = sweep_tmap_acc(h, ad.A, d, v);
+            ad.tmap_wb = sweep_tmap_wb(h, ad.W, d, v);
             CK(h, mixed ? gkm::launch_sweep_mixed_rows(d, v, ad, j0, j1, s) : gkm::launch_sweep_rows(d, v, ad, j0, j1, s));
         }
         CK(h, gkm::launch_halo_planes(A, fc, 3 + j0, 3 + j1, s));

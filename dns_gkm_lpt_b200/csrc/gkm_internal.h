@@ -85,7 +85,8 @@ struct SweepArgs {
                                     // at f1 (f0 = f1 = 0: the whole normal range)
     int skip_clock_init;            // 1: the clock's dt and next wave slot were set before the launch
     const void* tmap;               // FP64: tensor map of W for the slab copies (x, y: one slab; z: two)
-    const void* tmap_acc;           // FP64 z sweep: tensor map of A for the accumulator bricks (else null)
+    const void* tmap_acc;           // z sweep: tensor map of A for the accumulator bricks (else null)
+    const void* tmap_wb;            // mixed z sweep: tensor map of W for the FP64 state bricks (else null)
     int wait_probe;                 // test hook: make CTA (0, 0, 0)'s first bounded copy wait run out
 };
 

@@ -146,10 +146,9 @@ __host__ __device__ constexpr size_t sweep_ring_bytes()
 }
 
 // ring + reconstructions, then a per-thread FP64 staging area [5][threads] for the
-// accumulator of the thread's cell, fetched asynchronously while the flux is computed
-// the mixed x and z sweeps use neither the staging area nor the aligned ring (no tensor copies):
-// their ring and reconstructions alone (3 CTAs: 97.6 KB instead of 115 KB per SM, so more of the
-// SM's memory stays L1 for the z sweep's strided loads; 256^3 mixed sweeps -1.8 %)
+// accumulator of the thread's cell, fetched asynchronously while the flux is computed.
+// The mixed x sweep (and a mixed sweep without tensor maps) keeps its FP32 ring unaligned and
+// has no staging area.
 template <class T, int DIR>
 __host__ __device__ constexpr bool sweep_lean()
 {
@@ -174,18 +173,38 @@ __host__ __device__ constexpr int zland_elems()
 template <class T, int DIR>
 __host__ __device__ constexpr bool sweep_zpairs()
 {
-    return DIR == 2 && sizeof(T) == 8;
+    return DIR == 2;
+}
+// mixed x and y sweeps: each new slab lands in FP64 by one bulk tensor copy in a landing area, and the
+// threads convert it into the FP32 ring
+template <class T, int DIR>
+__host__ __device__ constexpr bool sweep_mland()
+{
+    return sizeof(T) == 4 && DIR != 2;
+}
+// the mixed z sweep's FP64 state of the updated cells (its ring holds FP32 copies) comes as bricks
+// too, else by direct loads
+template <class T>
+__host__ __device__ constexpr bool sweep_state_bricks()
+{
+    return sizeof(T) == 4;
 }
 
 template <class T, class Tile, int DIR = 1>
 __host__ __device__ constexpr size_t sweep_smem_bytes()
 {
-    if (sweep_lean<T, DIR>()) return sizeof(T) * (size_t)(kRing * slot_elems<T, Tile>() + 10 * Tile::WC);
-    // ring + reconstructions, 128 bytes of slack to align the bricks, two accumulator bricks, the
-    // slab landing area, three mbarriers
+    // z sweep: ring + reconstructions, 128 bytes of slack to align the bricks, two accumulator
+    // bricks, two bricks of the FP64 state (mixed form), the slab landing area, three mbarriers
     if (sweep_zpairs<T, DIR>())
-        return (sweep_ring_bytes<T, Tile>() + 128 + sizeof(double) * (2 * zbrick_elems<Tile>() + zland_elems<Tile>()) + 24 +
-                15) / 16 * 16;
+        return (sweep_ring_bytes<T, Tile>() + 128 +
+                sizeof(double) * ((sweep_state_bricks<T>() ? 4 : 2) * zbrick_elems<Tile>() + zland_elems<Tile>()) + 24 + 15) /
+               16 * 16;
+    // mixed x, y: ring + reconstructions, the y sweep's accumulator staging, slack, the landing area,
+    // one mbarrier
+    if (sweep_mland<T, DIR>())
+        return sweep_ring_bytes<T, Tile>() + (DIR == 1 ? sizeof(double) * 5 * (size_t)Tile::threads : 0) + 128 +
+               sizeof(double) * 5 * (size_t)Tile::WC + 16;
+    if (sweep_lean<T, DIR>()) return sizeof(T) * (size_t)(kRing * slot_elems<T, Tile>() + 10 * Tile::WC);
     return sweep_ring_bytes<T, Tile>() + sizeof(double) * 5 * (size_t)Tile::threads + 16;   // + mbarrier
 }
 
@@ -232,6 +251,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity,
     return false;
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// global -> shared bulk tensor copy completing on a barrier phase whose expected bytes were
+// already announced (by the tma_slab_load of the same phase)
+__device__ __forceinline__ void tma_box_load(unsigned dst, const void* tmap, int c0, int c1, int c2, unsigned bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(dst),
+        "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(0), "r"(bar)
+        : "memory");
+}
 // shared -> global bulk tensor copy of a box whose origin (c0, c1, c2, 0) is inside the tensor
 // (elements beyond its extent are not written), and the waits on such copies: until each has read
 // its shared-memory source, and until each has completed
@@ -316,16 +345,24 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     T* rec = ring + kRing * kSlot;
     constexpr bool kZPairs = sweep_zpairs<T, DIR>();
     constexpr int kZB = zbrick_elems<Tile>();
-    // FP64 z sweep: two accumulator bricks (128-byte aligned for the bulk copies), whose space also
-    // serves as the staging area, the slab landing area [q][a][b][2], then three mbarriers (the two
-    // bricks', the landing area's)
+    // z sweep: two accumulator bricks (128-byte aligned for the bulk copies), whose space also
+    // serves as the FP64 staging area, in the mixed form two bricks of the FP64 state, the slab
+    // landing area [q][a][b][2], then three mbarriers (the two bricks', the landing area's)
     double* stage =
         kZPairs ? reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw + sweep_ring_bytes<T, Tile>()) + 127) &
                                             ~uintptr_t(127))
                 : reinterpret_cast<double*>(smem_raw + sweep_ring_bytes<T, Tile>());   // [5][threads]
-    double* land = stage + 2 * kZB;
-    unsigned long long* bar =
-        reinterpret_cast<unsigned long long*>(kZPairs ? land + zland_elems<Tile>() : stage + 5 * kSweepThreads);
+    // every area a bulk tensor copy writes starts on a 128-byte boundary: the bricks' sizes keep it
+    static_assert(zbrick_elems<Tile>() * sizeof(double) % 128 == 0, "brick size breaks the 128-byte alignment");
+    double* wbr = stage + 2 * kZB;                                           // mixed z sweep: [2] FP64 state bricks
+    double* land = wbr + (sweep_state_bricks<T>() ? 2 * kZB : 0);             // [q][a][b][2]
+    // mixed x, y sweeps: the FP64 landing area [q][a][b] of one slab (after the y sweep's staging)
+    constexpr bool kMLand = sweep_mland<T, DIR>();
+    double* mland = reinterpret_cast<double*>(
+        (reinterpret_cast<uintptr_t>(smem_raw + sweep_ring_bytes<T, Tile>() + (DIR == 1 ? 40 * kSweepThreads : 0)) + 127) &
+        ~uintptr_t(127));
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(
+        kZPairs ? land + zland_elems<Tile>() : (kMLand ? mland + 5 * kWC : stage + 5 * kSweepThreads));
     const FieldConst& fc = a.fc;
     const int n = fc.n, nt = fc.nt;
     const long long nt3 = fc.nt3;
@@ -357,18 +394,39 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     // window, a box of the (k, i, j, q) tensor whose smem image is the slot's [q][a][b] layout)
     // with one bulk tensor copy completing on the mbarrier
     const bool use_tma = !kMixed && DIR != 2 && a.tmap != nullptr;
+    const bool mtma = kMLand && a.tmap != nullptr;   // mixed x / y: slabs land in FP64 by tensor copy
     // failure-detection test hook: the first CTA's first copy is expected with kProbeExtraBytes more
     // than it delivers, so its first wait (kProbePolls polls) runs out and raises status bit 1; the
     // CTA then retires the extra bytes and waits for the copy itself, which lands normally
     const bool probe = use_tma && a.wait_probe && bx == 0 && by == 0 && bz == 0;
     const unsigned bar_u32 = smem_u32(bar);
     unsigned tma_phase = 0;
-    if (use_tma) {
+    if (use_tma || mtma) {
         if (tid == 0) mbar_init(bar_u32);
         __syncthreads();
     }
 
     auto slot = [&](int f) { return ring + ((f + 12) % kRing) * kSlot; };
+    // one cell of a slab into its ring slot: the conserved values with the temperature, converted to
+    // the non-dimensional single-precision units in the mixed form
+    auto store_cell = [&](T* s, int c, double r, double m1, double m2, double m3, double E) {
+        if constexpr (kMixed) {
+            const double Tk = temperature<double>(r, m1, m2, m3, E, Phys<double>{fc.gam, fc.gm1, kR, fc.K});
+            s[0 * kWC + c] = T(r * fc.inv_rho_s);
+            s[1 * kWC + c] = T(m1 * fc.inv_m_s);
+            s[2 * kWC + c] = T(m2 * fc.inv_m_s);
+            s[3 * kWC + c] = T(m3 * fc.inv_m_s);
+            s[4 * kWC + c] = T(E * fc.inv_E_s);
+            s[5 * kWC + c] = T(Tk * fc.inv_T0);
+        } else {
+            s[0 * kWC + c] = r;
+            s[1 * kWC + c] = m1;
+            s[2 * kWC + c] = m2;
+            s[3 * kWC + c] = m3;
+            s[4 * kWC + c] = E;
+            s[5 * kWC + c] = temperature<double>(r, m1, m2, m3, E, ph);
+        }
+    };
     auto load_slab = [&](int f) {
         T* s = slot(f);
         for (int c = tid; c < kWC; c += kSweepThreads) {
@@ -376,31 +434,14 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             const int A = a0 + aa - 1, B = b0 + bb - 1;
             if (A > n || B > n) continue;
             const long long idx = (A + 3) * st.sA + (B + 3) * st.sB + (long long)(f + 3) * st.sn;
-            const double r = W[idx], m1 = W[nt3 + idx], m2 = W[2 * nt3 + idx], m3 = W[3 * nt3 + idx],
-                         E = W[4 * nt3 + idx];
-            if constexpr (kMixed) {
-                const double Tk = temperature<double>(r, m1, m2, m3, E, Phys<double>{fc.gam, fc.gm1, kR, fc.K});
-                s[0 * kWC + c] = T(r * fc.inv_rho_s);
-                s[1 * kWC + c] = T(m1 * fc.inv_m_s);
-                s[2 * kWC + c] = T(m2 * fc.inv_m_s);
-                s[3 * kWC + c] = T(m3 * fc.inv_m_s);
-                s[4 * kWC + c] = T(E * fc.inv_E_s);
-                s[5 * kWC + c] = T(Tk * fc.inv_T0);
-            } else {
-                s[0 * kWC + c] = r;
-                s[1 * kWC + c] = m1;
-                s[2 * kWC + c] = m2;
-                s[3 * kWC + c] = m3;
-                s[4 * kWC + c] = E;
-                s[5 * kWC + c] = temperature<double>(r, m1, m2, m3, E, ph);
-            }
+            store_cell(s, c, W[idx], W[nt3 + idx], W[2 * nt3 + idx], W[3 * nt3 + idx], W[4 * nt3 + idx]);
         }
     };
 
     // FP64: the slab of the next step travels global -> shared asynchronously during this step's
     // flux, straight into its ring slot (last read by this step's reconstruction); each thread
-    // forms the temperature of the cells it copied once its copies have landed.  (The mixed form
-    // converts while loading; an asynchronous landing area measured slower there.)
+    // forms the temperature of the cells it copied once its copies have landed.  (Without tensor
+    // maps the mixed form converts while loading.)
     auto issue_slab = [&](int f) {
         double* dst = reinterpret_cast<double*>(slot(f));
         for (int c = tid; c < kWC; c += kSweepThreads) {
@@ -438,7 +479,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     // written.  A cell whose partner lies in another segment (at most the first and the last of
     // each) is read and written directly, so no two CTAs store the same brick.
     const bool zslab = kZPairs && a.tmap != nullptr;
-    const bool zpair = kZPairs && a.tmap_acc != nullptr;
+    const bool zpair = kZPairs && a.tmap_acc != nullptr && (!sweep_state_bricks<T>() || a.tmap_wb != nullptr);
     const unsigned zbar = smem_u32(bar), lbar = zbar + 16u;
     unsigned zph = 0;   // bit b: the phase of brick buffer b's barrier awaited next
     unsigned lph = 0;   // the phase of the landing area's barrier awaited next
@@ -450,11 +491,26 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     auto zbuf = [](int f) { return ((f + 3) >> 1) & 1; };
     auto zload = [&](int pf) {   // the brick of the pair whose first cell is pf (one thread)
         const int b = zbuf(pf);
-        tma_slab_load(smem_u32(stage + b * kZB), a.tmap_acc, pf + 3, b0 + 3, a0 + 3, (unsigned)(kZB * sizeof(double)),
-                      zbar + 8u * b);
+        if constexpr (sweep_state_bricks<T>()) {   // the accumulator's and the FP64 state's bricks, one barrier phase
+            tma_slab_load(smem_u32(stage + b * kZB), a.tmap_acc, pf + 3, b0 + 3, a0 + 3,
+                          (unsigned)(2 * kZB * sizeof(double)), zbar + 8u * b);
+            tma_box_load(smem_u32(wbr + b * kZB), a.tmap_wb, pf + 3, b0 + 3, a0 + 3, zbar + 8u * b);
+        } else {
+            tma_slab_load(smem_u32(stage + b * kZB), a.tmap_acc, pf + 3, b0 + 3, a0 + 3,
+                          (unsigned)(kZB * sizeof(double)), zbar + 8u * b);
+        }
     };
     auto zslab_load = [&](int p) {   // planes p, p+1 (p + 3 even) of the window and its halo (one thread)
         tma_slab_load(smem_u32(land), a.tmap, p + 3, b0 + 2, a0 + 2, (unsigned)(zland_elems<Tile>() * sizeof(double)), lbar);
+    };
+    // mixed x / y: plane f from the FP64 landing area [q][a][b] into its ring slot
+    auto finish_slab_mland = [&](int f) {
+        T* s = slot(f);
+        for (int c = tid; c < kWC; c += kSweepThreads) {
+            const int aa = c / kWB, bb = c - aa * kWB;
+            if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
+            store_cell(s, c, mland[c], mland[kWC + c], mland[2 * kWC + c], mland[3 * kWC + c], mland[4 * kWC + c]);
+        }
     };
     // plane f from the landing area into its ring slot, with its temperature
     auto finish_slab_landed = [&](int f) {
@@ -463,14 +519,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
         for (int c = tid; c < kWC; c += kSweepThreads) {
             const int aa = c / kWB, bb = c - aa * kWB;
             if (a0 + aa - 1 > n || b0 + bb - 1 > n) continue;
-            const double r = L[2 * c], m1 = L[2 * (kWC + c)], m2 = L[2 * (2 * kWC + c)], m3 = L[2 * (3 * kWC + c)],
-                         E = L[2 * (4 * kWC + c)];
-            s[c] = r;
-            s[kWC + c] = m1;
-            s[2 * kWC + c] = m2;
-            s[3 * kWC + c] = m3;
-            s[4 * kWC + c] = E;
-            s[5 * kWC + c] = temperature<T>(r, m1, m2, m3, E, ph);
+            store_cell(s, c, L[2 * c], L[2 * (kWC + c)], L[2 * (2 * kWC + c)], L[2 * (3 * kWC + c)], L[2 * (4 * kWC + c)]);
         }
     };
     if (zpair || zslab) {
@@ -494,7 +543,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     bool bad = false;
 
     for (int f = f_begin - 1; f < f_end; f++) {
-        if (kMixed || f == f_begin - 1) {
+        if ((kMixed && !zslab && !mtma) || f == f_begin - 1) {
             load_slab(f + 3);
         } else {
             if (use_tma) {
@@ -502,6 +551,9 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                     if (!mbar_wait_bounded(bar_u32, tma_phase, kProbePolls)) atomicOr(&a.clock->status, 2);
                     if (tid == 0) mbar_complete_tx(bar_u32, kProbeExtraBytes);
                 }
+                if (!mbar_wait_bounded(bar_u32, tma_phase)) atomicOr(&a.clock->status, 2);
+                tma_phase ^= 1u;
+            } else if (mtma) {
                 if (!mbar_wait_bounded(bar_u32, tma_phase)) atomicOr(&a.clock->status, 2);
                 tma_phase ^= 1u;
             } else if (zslab) {
@@ -514,6 +566,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 cp_async_wait_all();
             }
             if (zslab) finish_slab_landed(f + 3);
+            else if (mtma) finish_slab_mland(f + 3);
             else finish_slab(f + 3);
         }
         __syncthreads();
@@ -637,7 +690,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             }
         }
         __syncthreads();
-        if (!kMixed && f + 1 < f_end) {
+        if (f + 1 < f_end) {
             if (use_tma) {
                 if (tid == 0) {
                     // box origin: window row a0-1, column b0-1 (ghost-layout +3), normal plane f+4
@@ -647,7 +700,13 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                                       ((probe && f == f_begin - 1) ? kProbeExtraBytes : 0u),
                                   bar_u32);
                 }
-            } else if (!zslab) {
+            } else if (mtma) {
+                if (tid == 0) {   // the FP64 slab of plane f+4 into the landing area, converted next face
+                    const int cb = b0 + 2, ca = a0 + 2, cn = f + 4 + 3;
+                    tma_slab_load(smem_u32(mland), a.tmap, cb, DIR == 0 ? cn : ca, DIR == 0 ? ca : cn,
+                                  (unsigned)(5 * kWC * sizeof(double)), bar_u32);
+                }
+            } else if (!kMixed && !zslab) {
                 issue_slab(f + 4);
             }
         }
@@ -727,8 +786,11 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                         double acc = zp ? zc[q * 2 * kTA * kTB]
                                         : ((kFetchA && !zpair) ? stage[q * kSweepThreads + tid] : a.A[q * nt3 + ci]);
                         double s = __dsub_rn(__dadd_rn(acc, F[q]), Fprev[q]);
-                        // the cell's FP64 state (the FP64 ring holds it; the mixed ring has FP32 copies)
-                        const double wq = kMixed ? W[q * nt3 + ci] : (double)wl[q * kWC + cc];
+                        // the cell's FP64 state (the FP64 ring holds it; the mixed ring has FP32 copies, so
+                        // the mixed form reads it from the pair's state brick, or directly)
+                        const double wq = kMixed ? ((sweep_state_bricks<T>() && zp) ? zc[(wbr - stage) + q * 2 * kTA * kTB]
+                                                                                    : W[q * nt3 + ci])
+                                                 : (double)wl[q * kWC + cc];
                         wn[q] = __dsub_rn(wq, __dmul_rn(fc.inv_dx, s));
                         if (zp) zc[q * 2 * kTA * kTB] = wn[q];
                         else a.A[q * nt3 + ci] = wn[q];
@@ -761,7 +823,7 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
         if (tid == 0 && m > 0.0) atomicMax(&a.clock->wave[a.parity ^ 1], (unsigned long long)__double_as_longlong(m));
         if (bad) atomicOr(&a.clock->status, 1);
     }
-    if (use_tma) {   // every wait on the barrier has returned: retire it (a persistent CTA re-initialises it)
+    if (use_tma || mtma) {   // every wait on the barrier has returned: retire it (a persistent CTA re-initialises it)
         __syncthreads();
         if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar_u32) : "memory");
     }
@@ -803,13 +865,14 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
         const int bz = (int)(local % nseg);
         const long long t = local / nseg;
         SweepArgs a;
-        // FP64: the member's tensor maps (4 per buffer and window variant: x slab, y slab, z
-        // accumulator brick, z slab box) of the buffer read and, for the z sweep, the buffer written;
-        // variant 1 = 16x16 windows
+        // the member's tensor maps (4 per buffer and window variant: x slab, y slab, z brick, z slab
+        // box) of the buffer read and, for the z sweep, the buffer written; variant 1 = 16x16 windows
+        // (FP64 only; the mixed form has one window)
         constexpr int kVariant = (sizeof(T) == 8 && Tile::TA == 16) ? 1 : 0;
-        const bool maps = sizeof(T) == 8 && md.tmaps;
+        const bool maps = md.tmaps != nullptr;
         a.tmap = maps ? md.tmaps + 128 * ((parity * kSweepVariants64 + kVariant) * 4 + (DIR == 2 ? 3 : DIR)) : nullptr;
         a.tmap_acc = (maps && DIR == 2) ? md.tmaps + 128 * (((parity ^ 1) * kSweepVariants64 + kVariant) * 4 + 2) : nullptr;
+        a.tmap_wb = (maps && DIR == 2) ? md.tmaps + 128 * ((parity * kSweepVariants64 + kVariant) * 4 + 2) : nullptr;
         a.tile_a0 = 0;
         a.f0 = 0;
         a.f1 = 0;

@@ -29,13 +29,15 @@ cudaError_t launch_one_mixed(const SweepArgs& a, int nseg, cudaStream_t s)
 cudaError_t sweep_mixed_prepare()
 {
     using Tile = SweepTile32a;
-    const int bytes = (int)sweep_detail::sweep_smem_bytes<float, Tile>();
-    cudaError_t e =
-        cudaFuncSetAttribute(sweep_kernel<0, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    using sweep_detail::sweep_smem_bytes;
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<0, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sweep_smem_bytes<float, Tile, 0>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<1, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(sweep_kernel<1, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sweep_smem_bytes<float, Tile, 1>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<2, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(sweep_kernel<2, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sweep_smem_bytes<float, Tile, 2>());
     if (e == cudaSuccess) e = set_ensemble_smem<float, Tile>();
     return e;
 }
