@@ -189,6 +189,14 @@ __host__ __device__ constexpr bool sweep_state_bricks()
 {
     return sizeof(T) == 4;
 }
+// brick buffers of the z sweep: two (the next pair's brick requested one cell before the current
+// pair's store), or one (requested after that store has read it) where shared memory decides how
+// many CTAs an SM holds (the mixed form: three CTAs per SM instead of two)
+template <class T>
+__host__ __device__ constexpr int sweep_zbufs()
+{
+    return sizeof(T) == 4 ? 1 : 2;
+}
 
 template <class T, class Tile, int DIR = 1>
 __host__ __device__ constexpr size_t sweep_smem_bytes()
@@ -197,7 +205,9 @@ __host__ __device__ constexpr size_t sweep_smem_bytes()
     // bricks, two bricks of the FP64 state (mixed form), the slab landing area, three mbarriers
     if (sweep_zpairs<T, DIR>())
         return (sweep_ring_bytes<T, Tile>() + 128 +
-                sizeof(double) * ((sweep_state_bricks<T>() ? 4 : 2) * zbrick_elems<Tile>() + zland_elems<Tile>()) + 24 + 15) /
+                sizeof(double) * ((sweep_state_bricks<T>() ? 2 : 1) * sweep_zbufs<T>() * zbrick_elems<Tile>() +
+                                  zland_elems<Tile>()) +
+                24 + 15) /
                16 * 16;
     // mixed x, y: ring + reconstructions, the y sweep's accumulator staging, slack, the landing area,
     // one mbarrier
@@ -354,8 +364,9 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 : reinterpret_cast<double*>(smem_raw + sweep_ring_bytes<T, Tile>());   // [5][threads]
     // every area a bulk tensor copy writes starts on a 128-byte boundary: the bricks' sizes keep it
     static_assert(zbrick_elems<Tile>() * sizeof(double) % 128 == 0, "brick size breaks the 128-byte alignment");
-    double* wbr = stage + 2 * kZB;                                           // mixed z sweep: [2] FP64 state bricks
-    double* land = wbr + (sweep_state_bricks<T>() ? 2 * kZB : 0);             // [q][a][b][2]
+    constexpr int kZBufs = sweep_zbufs<T>();
+    double* wbr = stage + kZBufs * kZB;                                       // mixed z sweep: FP64 state bricks
+    double* land = wbr + (sweep_state_bricks<T>() ? kZBufs * kZB : 0);        // [q][a][b][2]
     // mixed x, y sweeps: the FP64 landing area [q][a][b] of one slab (after the y sweep's staging)
     constexpr bool kMLand = sweep_mland<T, DIR>();
     double* mland = reinterpret_cast<double*>(
@@ -488,7 +499,8 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
         const int p = first_of_pair(f) ? f + 1 : f - 1;
         return p >= f_begin && p < f_end;
     };
-    auto zbuf = [](int f) { return ((f + 3) >> 1) & 1; };
+    auto zbuf = [](int f) { return kZBufs == 2 ? ((f + 3) >> 1) & 1 : 0; };
+    const int pf0 = first_of_pair(f_begin) ? f_begin : f_begin + 1;   // the segment's first pair
     auto zload = [&](int pf) {   // the brick of the pair whose first cell is pf (one thread)
         const int b = zbuf(pf);
         if constexpr (sweep_state_bricks<T>()) {   // the accumulator's and the FP64 state's bricks, one barrier phase
@@ -529,7 +541,6 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             mbar_init(lbar);
         }
         __syncthreads();
-        const int pf0 = first_of_pair(f_begin) ? f_begin : f_begin + 1;
         if (tid == 0 && zpair && pf0 + 1 < f_end) zload(pf0);
         // the first plane not loaded directly, f_begin + 3, and its partner
         if (tid == 0 && zslab) zslab_load(first_of_pair(f_begin + 3) ? f_begin + 3 : f_begin + 2);
@@ -576,10 +587,14 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
             // the pair the previous cell completed goes out (its writes were fenced before the barrier)
             if (!first_of_pair(f - 1) && paired(f - 1))
                 tma_box_store(a.tmap_acc, f + 1, b0 + 3, a0 + 3, smem_u32(stage + zbuf(f - 1) * kZB));
-            // the next pair comes in, into the buffer whose store left one cell ago
-            if (!first_of_pair(f) && paired(f) && f + 2 < f_end) {
+            if (kZBufs == 2) {   // the next pair comes in, into the buffer whose store left one cell ago
+                if (!first_of_pair(f) && paired(f) && f + 2 < f_end) {
+                    bulk_wait_read();
+                    zload(f + 1);
+                }
+            } else if (first_of_pair(f) && f + 1 < f_end && f != pf0) {   // this cell's pair, once the store has read the buffer
                 bulk_wait_read();
-                zload(f + 1);
+                zload(f);
             }
         }
         // reconstruct every face of the window once (the reference repeats this 5x per face)
