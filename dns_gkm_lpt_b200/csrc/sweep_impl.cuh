@@ -474,7 +474,42 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
         }
     };
 
-    for (int f = f_begin - 3; f < f_begin + 2; f++) load_slab(f);
+    // the segment's first six slabs arrive together (FP64 x / y sweeps with a tensor map: six bulk
+    // tensor copies completing on one barrier phase), instead of six rounds of loads
+    if (use_tma) {
+        if (tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar_u32),
+                         "r"((unsigned)(6 * 5 * kWC * sizeof(double)))
+                         : "memory");
+            for (int f = f_begin - 3; f < f_begin + 3; f++)
+                tma_box_load(smem_u32(slot(f)), a.tmap, b0 + 2, DIR == 0 ? f + 3 : a0 + 2, DIR == 0 ? a0 + 2 : f + 3,
+                             bar_u32);
+        }
+        if (!mbar_wait_bounded(bar_u32, tma_phase)) atomicOr(&a.clock->status, 2);
+        tma_phase ^= 1u;
+        for (int f = f_begin - 3; f < f_begin + 3; f++) finish_slab(f);
+    } else if (!kMixed) {
+        // FP64 otherwise (the z sweep, odd nt): the first six slabs by cp.async, one wait for all
+        for (int f = f_begin - 3; f < f_begin + 3; f++) issue_slab(f);
+        cp_async_wait_all();
+        for (int f = f_begin - 3; f < f_begin + 3; f++) finish_slab(f);
+    } else {
+        // mixed form: the first six slabs by one round of loads per cell (30 in flight), then converted
+        for (int c = tid; c < kWC; c += kSweepThreads) {
+            const int aa = c / kWB, bb = c - aa * kWB;
+            const int A = a0 + aa - 1, B = b0 + bb - 1;
+            if (A > n || B > n) continue;
+            const long long idx0 = (A + 3) * st.sA + (B + 3) * st.sB;
+            double v[6][5];
+#pragma unroll
+            for (int p = 0; p < 6; p++)
+#pragma unroll
+                for (int q = 0; q < 5; q++) v[p][q] = W[q * nt3 + idx0 + (long long)(f_begin + p) * st.sn];
+#pragma unroll
+            for (int p = 0; p < 6; p++) store_cell(slot(f_begin - 3 + p), c, v[p][0], v[p][1], v[p][2], v[p][3], v[p][4]);
+        }
+    }
 
     // FP64 z sweep.  Its normal k is the contiguous axis, so one value per window cell and plane is
     // 8 bytes of a different 128-byte line; the window's 1,620 lines per plane (16 x 16 windows)
@@ -554,7 +589,9 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     bool bad = false;
 
     for (int f = f_begin - 1; f < f_end; f++) {
-        if ((kMixed && !zslab && !mtma) || f == f_begin - 1) {
+        if (f == f_begin - 1) {
+            // slab f + 3 came with the first six
+        } else if (kMixed && !zslab && !mtma) {
             load_slab(f + 3);
         } else {
             if (use_tma) {

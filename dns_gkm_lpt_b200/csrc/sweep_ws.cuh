@@ -121,23 +121,6 @@ __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int b
         const int ptid = tid - kConsumers;
         const bool probe = use_tma && a.wait_probe && bx == 0 && by == 0 && bz == 0;
         unsigned tma_phase = 0;
-        auto load_slab = [&](int f) {
-            T* s = slot(f);
-            for (int c = ptid; c < kWC; c += kProducers) {
-                const int aa = c / kWB, bb = c - aa * kWB;
-                const int A = a0 + aa - 1, B = b0 + bb - 1;
-                if (A > n || B > n) continue;
-                const long long idx = (A + 3) * st.sA + (B + 3) * st.sB + (long long)(f + 3) * st.sn;
-                const double r = W[idx], m1 = W[nt3 + idx], m2 = W[2 * nt3 + idx], m3 = W[3 * nt3 + idx],
-                             E = W[4 * nt3 + idx];
-                s[0 * kWC + c] = r;
-                s[1 * kWC + c] = m1;
-                s[2 * kWC + c] = m2;
-                s[3 * kWC + c] = m3;
-                s[4 * kWC + c] = E;
-                s[5 * kWC + c] = temperature<double>(r, m1, m2, m3, E, ph);
-            }
-        };
         auto issue_slab = [&](int f) {
             double* dst = slot(f);
             for (int c = ptid; c < kWC; c += kProducers) {
@@ -158,7 +141,24 @@ __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int b
                 s[5 * kWC + c] = temperature<T>(s[c], s[kWC + c], s[2 * kWC + c], s[3 * kWC + c], s[4 * kWC + c], ph);
             }
         };
-        for (int f = f_begin - 3; f < f_begin + 3; f++) load_slab(f);
+        if (use_tma) {   // the segment's first six slabs as six bulk tensor copies on one barrier phase
+            if (ptid == 0) {
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar_tma),
+                             "r"((unsigned)(6 * 5 * kWC * sizeof(double)))
+                             : "memory");
+                for (int f = f_begin - 3; f < f_begin + 3; f++)
+                    tma_box_load(smem_u32(slot(f)), a.tmap, b0 + 2, DIR == 0 ? f + 3 : a0 + 2, DIR == 0 ? a0 + 2 : f + 3,
+                                 bar_tma);
+            }
+            if (!mbar_wait_bounded(bar_tma, tma_phase)) timed_out = true;
+            tma_phase ^= 1u;
+            for (int f = f_begin - 3; f < f_begin + 3; f++) finish_slab(f);
+        } else {   // per-element cp.async, one wait for all six
+            for (int f = f_begin - 3; f < f_begin + 3; f++) issue_slab(f);
+            cp_async_wait_all();
+            for (int f = f_begin - 3; f < f_begin + 3; f++) finish_slab(f);
+        }
         for (int k = 0; k < nf; k++) {
             const int f = f_begin - 1 + k;
             if (k > 0) {   // slab f + 3, issued at the end of the previous face
