@@ -165,7 +165,8 @@ cudaError_t launch_one(const SweepArgs& a, int nseg, cudaStream_t s)
 {
     dim3 grid((a.fc.n + Tile::TB - 1) / Tile::TB, (a.fc.n + Tile::TA - 1) / Tile::TA, nseg);
     dim3 block(Tile::TB, Tile::TA);
-    sweep_kernel<DIR, double, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<double, Tile, DIR>(), s>>>(a);
+    if constexpr (DIR == 2) launch_z<double, Tile>(a, grid, block, sweep_detail::sweep_smem_bytes<double, Tile, 2>(), s);
+    else sweep_kernel<DIR, double, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<double, Tile, DIR>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -178,9 +179,7 @@ cudaError_t set_smem()
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(sweep_kernel<1, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sweep_smem_bytes<double, Tile, 1>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<2, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sweep_smem_bytes<double, Tile, 2>());
+    if (e == cudaSuccess) e = set_z_smem<double, Tile>();
     return e;
 }
 

@@ -337,10 +337,15 @@ __device__ __forceinline__ void halo_cell(double* __restrict__ W, const FieldCon
     for (int q = 0; q < 5; q++) W[q * nt3 + dst] = W[q * nt3 + src];
 }
 
+// z sweeps: which data movement a kernel is compiled for.  The single-cube launches pick the form
+// by whether the handle has tensor maps, so each kernel holds only its own path; the ensemble's
+// persistent kernel serves members with and without maps and decides per item.
+constexpr int kZRuntime = 0, kZMaps = 1, kZNoMaps = 2;
+
 // One CTA's work: the window (bx, by) of faces, segment bz along the normal.
 // Called once per CTA by sweep_kernel and once per work item by the
 // persistent ensemble kernel; every thread of the CTA takes the same path.
-template <int DIR, class T, class Tile>
+template <int DIR, class T, class Tile, int ZM = kZRuntime>
 __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, int bz, unsigned char* smem_raw)
 {
     using namespace sweep_detail;
@@ -524,8 +529,9 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     // starts), updated in shared memory by its two cells and stored once the second cell is
     // written.  A cell whose partner lies in another segment (at most the first and the last of
     // each) is read and written directly, so no two CTAs store the same brick.
-    const bool zslab = kZPairs && a.tmap != nullptr;
-    const bool zpair = kZPairs && a.tmap_acc != nullptr && (!sweep_state_bricks<T>() || a.tmap_wb != nullptr);
+    const bool zslab = kZPairs && (ZM == kZMaps || (ZM == kZRuntime && a.tmap != nullptr));
+    const bool zpair = kZPairs && (ZM == kZMaps || (ZM == kZRuntime && a.tmap_acc != nullptr &&
+                                                    (!sweep_state_bricks<T>() || a.tmap_wb != nullptr)));
     const unsigned zbar = smem_u32(bar), lbar = zbar + 16u;
     unsigned zph = 0;   // bit b: the phase of brick buffer b's barrier awaited next
     unsigned lph = 0;   // the phase of the landing area's barrier awaited next
@@ -881,11 +887,34 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     }
 }
 
-template <int DIR, class T, class Tile>
+template <int DIR, class T, class Tile, int ZM = kZRuntime>
 __global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    sweep_block<DIR, T, Tile>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
+    sweep_block<DIR, T, Tile, ZM>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
+}
+
+// the z kernel form for the maps a launch carries (the mixed form also needs its state map)
+template <class T>
+__host__ __device__ inline bool z_maps_present(const SweepArgs& a)
+{
+    return a.tmap != nullptr && a.tmap_acc != nullptr && (!sweep_detail::sweep_state_bricks<T>() || a.tmap_wb != nullptr);
+}
+template <class T, class Tile>
+void launch_z(const SweepArgs& a, dim3 grid, dim3 block, size_t smem, cudaStream_t s)
+{
+    if (z_maps_present<T>(a)) sweep_kernel<2, T, Tile, kZMaps><<<grid, block, smem, s>>>(a);
+    else sweep_kernel<2, T, Tile, kZNoMaps><<<grid, block, smem, s>>>(a);
+}
+template <class T, class Tile>
+cudaError_t set_z_smem()
+{
+    const int bytes = (int)sweep_detail::sweep_smem_bytes<T, Tile, 2>();
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<2, T, Tile, kZMaps>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_kernel<2, T, Tile, kZNoMaps>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
 }
 
 // Persistent form for an ensemble: a fixed grid of CTAs takes the flattened
@@ -964,7 +993,7 @@ cudaError_t launch_sweep_rows_t(int dir, SweepArgs a, int j0, int j1, cudaStream
     a.tile_a0 = j0 / Tile::TA;
     const dim3 grid(gb, (j1 + Tile::TA - 1) / Tile::TA - a.tile_a0, (n + a.seg_len - 1) / a.seg_len);
     if (dir == 0) sweep_kernel<0, T, Tile><<<grid, block, smem0, s>>>(a);
-    else sweep_kernel<2, T, Tile><<<grid, block, smem2, s>>>(a);
+    else launch_z<T, Tile>(a, grid, block, smem2, s);
     return cudaGetLastError();
 }
 

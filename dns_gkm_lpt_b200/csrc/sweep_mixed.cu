@@ -20,7 +20,8 @@ cudaError_t launch_one_mixed(const SweepArgs& a, int nseg, cudaStream_t s)
     using Tile = SweepTile32a;
     dim3 grid((a.fc.n + Tile::TB - 1) / Tile::TB, (a.fc.n + Tile::TA - 1) / Tile::TA, nseg);
     dim3 block(Tile::TB, Tile::TA);
-    sweep_kernel<DIR, float, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<float, Tile, DIR>(), s>>>(a);
+    if constexpr (DIR == 2) launch_z<float, Tile>(a, grid, block, sweep_detail::sweep_smem_bytes<float, Tile, 2>(), s);
+    else sweep_kernel<DIR, float, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<float, Tile, DIR>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -35,9 +36,7 @@ cudaError_t sweep_mixed_prepare()
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(sweep_kernel<1, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sweep_smem_bytes<float, Tile, 1>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<2, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sweep_smem_bytes<float, Tile, 2>());
+    if (e == cudaSuccess) e = set_z_smem<float, Tile>();
     if (e == cudaSuccess) e = set_ensemble_smem<float, Tile>();
     return e;
 }
