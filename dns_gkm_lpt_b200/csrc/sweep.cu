@@ -141,22 +141,30 @@ __global__ void weno_faces_kernel(const double* __restrict__ s, long long n, Phy
 // its warpgroups' setmaxnreg split draws on (a smaller launch count would leave them waiting)
 bool g_ws_ready = false;
 
-template <int DIR>
+template <int DIR, int MM>
 cudaError_t ws_check(bool& ok)
 {
     cudaFuncAttributes at;
-    cudaError_t e = cudaFuncGetAttributes(&at, sweep_ws_kernel<DIR, SweepTile64b>);
+    cudaError_t e = cudaFuncGetAttributes(&at, sweep_ws_kernel<DIR, SweepTile64b, MM>);
     if (e != cudaSuccess) return e;
     ok = ok && at.numRegs == 168;
-    return cudaFuncSetAttribute(sweep_ws_kernel<DIR, SweepTile64b>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(sweep_ws_kernel<DIR, SweepTile64b, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sweep_ws_detail::ws_smem_bytes<SweepTile64b>());
 }
 
+// x, y: the form with tensor copies when the launch carries a map; z: per-element copies
 template <int DIR>
 cudaError_t launch_ws(SweepArgs a, dim3 grid, cudaStream_t s)
 {
-    sweep_ws_kernel<DIR, SweepTile64b>
-        <<<grid, sweep_ws_detail::kThreads, sweep_ws_detail::ws_smem_bytes<SweepTile64b>(), s>>>(a);
+    constexpr unsigned th = sweep_ws_detail::kThreads;
+    const size_t smem = sweep_ws_detail::ws_smem_bytes<SweepTile64b>();
+    if constexpr (DIR != 2) {
+        if (a.tmap != nullptr) {
+            sweep_ws_kernel<DIR, SweepTile64b, kMapsOn><<<grid, th, smem, s>>>(a);
+            return cudaGetLastError();
+        }
+    }
+    sweep_ws_kernel<DIR, SweepTile64b, kMapsOff><<<grid, th, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -165,21 +173,16 @@ cudaError_t launch_one(const SweepArgs& a, int nseg, cudaStream_t s)
 {
     dim3 grid((a.fc.n + Tile::TB - 1) / Tile::TB, (a.fc.n + Tile::TA - 1) / Tile::TA, nseg);
     dim3 block(Tile::TB, Tile::TA);
-    if constexpr (DIR == 2) launch_z<double, Tile>(a, grid, block, sweep_detail::sweep_smem_bytes<double, Tile, 2>(), s);
-    else sweep_kernel<DIR, double, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<double, Tile, DIR>(), s>>>(a);
+    launch_form<DIR, double, Tile>(a, grid, block, s);
     return cudaGetLastError();
 }
 
 template <class Tile>
 cudaError_t set_smem()
 {
-    using sweep_detail::sweep_smem_bytes;
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<0, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sweep_smem_bytes<double, Tile, 0>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<1, double, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sweep_smem_bytes<double, Tile, 1>());
-    if (e == cudaSuccess) e = set_z_smem<double, Tile>();
+    cudaError_t e = set_form_smem<0, double, Tile>();
+    if (e == cudaSuccess) e = set_form_smem<1, double, Tile>();
+    if (e == cudaSuccess) e = set_form_smem<2, double, Tile>();
     return e;
 }
 
@@ -214,9 +217,11 @@ cudaError_t sweep_prepare()
     if (e == cudaSuccess) e = set_ensemble_smem<double, SweepTile64a>();
     if (e == cudaSuccess) e = set_ensemble_smem<double, SweepTile64b>();
     bool ok = true;
-    if (e == cudaSuccess) e = ws_check<0>(ok);
-    if (e == cudaSuccess) e = ws_check<1>(ok);
-    if (e == cudaSuccess) e = ws_check<2>(ok);
+    if (e == cudaSuccess) e = ws_check<0, kMapsOn>(ok);
+    if (e == cudaSuccess) e = ws_check<0, kMapsOff>(ok);
+    if (e == cudaSuccess) e = ws_check<1, kMapsOn>(ok);
+    if (e == cudaSuccess) e = ws_check<1, kMapsOff>(ok);
+    if (e == cudaSuccess) e = ws_check<2, kMapsOff>(ok);
     g_ws_ready = e == cudaSuccess && ok;
     return e;
 }

@@ -337,15 +337,16 @@ __device__ __forceinline__ void halo_cell(double* __restrict__ W, const FieldCon
     for (int q = 0; q < 5; q++) W[q * nt3 + dst] = W[q * nt3 + src];
 }
 
-// z sweeps: which data movement a kernel is compiled for.  The single-cube launches pick the form
-// by whether the handle has tensor maps, so each kernel holds only its own path; the ensemble's
-// persistent kernel serves members with and without maps and decides per item.
-constexpr int kZRuntime = 0, kZMaps = 1, kZNoMaps = 2;
+// Which data movement a sweep kernel is compiled for: tensor copies (the handle has tensor maps)
+// or per-element copies (odd nt).  The single-cube launches pick the form by the maps a launch
+// carries, so each kernel holds only its own path; the ensemble's persistent kernel serves
+// members with and without maps and decides per item.
+constexpr int kMapsRuntime = 0, kMapsOn = 1, kMapsOff = 2;
 
 // One CTA's work: the window (bx, by) of faces, segment bz along the normal.
 // Called once per CTA by sweep_kernel and once per work item by the
 // persistent ensemble kernel; every thread of the CTA takes the same path.
-template <int DIR, class T, class Tile, int ZM = kZRuntime>
+template <int DIR, class T, class Tile, int MM = kMapsRuntime>
 __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, int bz, unsigned char* smem_raw)
 {
     using namespace sweep_detail;
@@ -409,8 +410,9 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     // FP64 x and y sweeps with a tensor map: one thread moves each new slab (5 components of the
     // window, a box of the (k, i, j, q) tensor whose smem image is the slot's [q][a][b] layout)
     // with one bulk tensor copy completing on the mbarrier
-    const bool use_tma = !kMixed && DIR != 2 && a.tmap != nullptr;
-    const bool mtma = kMLand && a.tmap != nullptr;   // mixed x / y: slabs land in FP64 by tensor copy
+    const bool maps = MM == kMapsOn || (MM == kMapsRuntime && a.tmap != nullptr);
+    const bool use_tma = !kMixed && DIR != 2 && maps;
+    const bool mtma = kMLand && maps;   // mixed x / y: slabs land in FP64 by tensor copy
     // failure-detection test hook: the first CTA's first copy is expected with kProbeExtraBytes more
     // than it delivers, so its first wait (kProbePolls polls) runs out and raises status bit 1; the
     // CTA then retires the extra bytes and waits for the copy itself, which lands normally
@@ -529,9 +531,9 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     // starts), updated in shared memory by its two cells and stored once the second cell is
     // written.  A cell whose partner lies in another segment (at most the first and the last of
     // each) is read and written directly, so no two CTAs store the same brick.
-    const bool zslab = kZPairs && (ZM == kZMaps || (ZM == kZRuntime && a.tmap != nullptr));
-    const bool zpair = kZPairs && (ZM == kZMaps || (ZM == kZRuntime && a.tmap_acc != nullptr &&
-                                                    (!sweep_state_bricks<T>() || a.tmap_wb != nullptr)));
+    const bool zslab = kZPairs && (MM == kMapsOn || (MM == kMapsRuntime && a.tmap != nullptr));
+    const bool zpair = kZPairs && (MM == kMapsOn || (MM == kMapsRuntime && a.tmap_acc != nullptr &&
+                                                     (!sweep_state_bricks<T>() || a.tmap_wb != nullptr)));
     const unsigned zbar = smem_u32(bar), lbar = zbar + 16u;
     unsigned zph = 0;   // bit b: the phase of brick buffer b's barrier awaited next
     unsigned lph = 0;   // the phase of the landing area's barrier awaited next
@@ -887,33 +889,36 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     }
 }
 
-template <int DIR, class T, class Tile, int ZM = kZRuntime>
+template <int DIR, class T, class Tile, int MM = kMapsRuntime>
 __global__ void __launch_bounds__(Tile::threads, Tile::ctas) sweep_kernel(SweepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    sweep_block<DIR, T, Tile, ZM>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
+    sweep_block<DIR, T, Tile, MM>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
 }
 
-// the z kernel form for the maps a launch carries (the mixed form also needs its state map)
+// the kernel form for the maps a launch carries (the z sweep needs the accumulator's too, the mixed
+// z sweep also the state's)
 template <class T>
-__host__ __device__ inline bool z_maps_present(const SweepArgs& a)
+__host__ __device__ inline bool maps_present(int dir, const SweepArgs& a)
 {
+    if (dir != 2) return a.tmap != nullptr;
     return a.tmap != nullptr && a.tmap_acc != nullptr && (!sweep_detail::sweep_state_bricks<T>() || a.tmap_wb != nullptr);
 }
-template <class T, class Tile>
-void launch_z(const SweepArgs& a, dim3 grid, dim3 block, size_t smem, cudaStream_t s)
+template <int DIR, class T, class Tile>
+void launch_form(const SweepArgs& a, dim3 grid, dim3 block, cudaStream_t s)
 {
-    if (z_maps_present<T>(a)) sweep_kernel<2, T, Tile, kZMaps><<<grid, block, smem, s>>>(a);
-    else sweep_kernel<2, T, Tile, kZNoMaps><<<grid, block, smem, s>>>(a);
+    const size_t smem = sweep_detail::sweep_smem_bytes<T, Tile, DIR>();
+    if (maps_present<T>(DIR, a)) sweep_kernel<DIR, T, Tile, kMapsOn><<<grid, block, smem, s>>>(a);
+    else sweep_kernel<DIR, T, Tile, kMapsOff><<<grid, block, smem, s>>>(a);
 }
-template <class T, class Tile>
-cudaError_t set_z_smem()
+template <int DIR, class T, class Tile>
+cudaError_t set_form_smem()
 {
-    const int bytes = (int)sweep_detail::sweep_smem_bytes<T, Tile, 2>();
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<2, T, Tile, kZMaps>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const int bytes = (int)sweep_detail::sweep_smem_bytes<T, Tile, DIR>();
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIR, T, Tile, kMapsOn>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<2, T, Tile, kZNoMaps>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(sweep_kernel<DIR, T, Tile, kMapsOff>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return e;
 }
 
@@ -978,22 +983,20 @@ cudaError_t launch_sweep_rows_t(int dir, SweepArgs a, int j0, int j1, cudaStream
     const int n = a.fc.n;
     if (j0 < 0 || j1 > n || j0 >= j1) return cudaErrorInvalidValue;
     const int gb = (n + Tile::TB - 1) / Tile::TB;
-    const size_t smem = sweep_detail::sweep_smem_bytes<T, Tile, 1>();
-    const size_t smem0 = sweep_detail::sweep_smem_bytes<T, Tile, 0>(), smem2 = sweep_detail::sweep_smem_bytes<T, Tile, 2>();
     const dim3 block(Tile::TB, Tile::TA);
     if (dir == 1) {
         if (a.seg_len < 1) return cudaErrorInvalidValue;
         a.f0 = j0;
         a.f1 = j1;
         const dim3 grid(gb, (n + Tile::TA - 1) / Tile::TA, (j1 - j0 + a.seg_len - 1) / a.seg_len);
-        sweep_kernel<1, T, Tile><<<grid, block, smem, s>>>(a);
+        launch_form<1, T, Tile>(a, grid, block, s);
         return cudaGetLastError();
     }
     if (j0 % Tile::TA) return cudaErrorInvalidValue;
     a.tile_a0 = j0 / Tile::TA;
     const dim3 grid(gb, (j1 + Tile::TA - 1) / Tile::TA - a.tile_a0, (n + a.seg_len - 1) / a.seg_len);
-    if (dir == 0) sweep_kernel<0, T, Tile><<<grid, block, smem0, s>>>(a);
-    else launch_z<T, Tile>(a, grid, block, smem2, s);
+    if (dir == 0) launch_form<0, T, Tile>(a, grid, block, s);
+    else launch_form<2, T, Tile>(a, grid, block, s);
     return cudaGetLastError();
 }
 

@@ -20,8 +20,7 @@ cudaError_t launch_one_mixed(const SweepArgs& a, int nseg, cudaStream_t s)
     using Tile = SweepTile32a;
     dim3 grid((a.fc.n + Tile::TB - 1) / Tile::TB, (a.fc.n + Tile::TA - 1) / Tile::TA, nseg);
     dim3 block(Tile::TB, Tile::TA);
-    if constexpr (DIR == 2) launch_z<float, Tile>(a, grid, block, sweep_detail::sweep_smem_bytes<float, Tile, 2>(), s);
-    else sweep_kernel<DIR, float, Tile><<<grid, block, sweep_detail::sweep_smem_bytes<float, Tile, DIR>(), s>>>(a);
+    launch_form<DIR, float, Tile>(a, grid, block, s);
     return cudaGetLastError();
 }
 
@@ -30,13 +29,9 @@ cudaError_t launch_one_mixed(const SweepArgs& a, int nseg, cudaStream_t s)
 cudaError_t sweep_mixed_prepare()
 {
     using Tile = SweepTile32a;
-    using sweep_detail::sweep_smem_bytes;
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<0, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sweep_smem_bytes<float, Tile, 0>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(sweep_kernel<1, float, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sweep_smem_bytes<float, Tile, 1>());
-    if (e == cudaSuccess) e = set_z_smem<float, Tile>();
+    cudaError_t e = set_form_smem<0, float, Tile>();
+    if (e == cudaSuccess) e = set_form_smem<1, float, Tile>();
+    if (e == cudaSuccess) e = set_form_smem<2, float, Tile>();
     if (e == cudaSuccess) e = set_ensemble_smem<float, Tile>();
     return e;
 }

@@ -65,7 +65,7 @@ __host__ __device__ constexpr size_t ws_smem_bytes()
 
 }  // namespace sweep_ws_detail
 
-template <int DIR, class Tile>
+template <int DIR, class Tile, int MM>
 __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int by, int bz, unsigned char* smem_raw)
 {
     using namespace sweep_detail;
@@ -99,7 +99,7 @@ __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int b
     }
     if (f_begin >= f_end) return;
 
-    const bool use_tma = DIR != 2 && a.tmap != nullptr;
+    const bool use_tma = DIR != 2 && (MM == kMapsOn || (MM == kMapsRuntime && a.tmap != nullptr));
     if (tid == 0) {
         mbar_init_count(bar_tma, 1);
         for (int b = 0; b < 2; b++) {
@@ -338,11 +338,12 @@ __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int b
         for (int b = 0; b < 5; b++) asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar_tma + 8 * b) : "memory");
 }
 
-template <int DIR, class Tile>
+// MM: compiled for tensor copies of the slabs (x, y sweeps with maps) or per-element copies
+template <int DIR, class Tile, int MM>
 __global__ void __launch_bounds__(sweep_ws_detail::kThreads, 1) sweep_ws_kernel(SweepArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    sweep_block_ws<DIR, Tile>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
+    sweep_block_ws<DIR, Tile, MM>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
 }
 
 }  // namespace gkm
