@@ -16,7 +16,9 @@ does not shard: no inter-GPU exchange); value sums all ranks over the slowest
 rank's time.
 
 "forms" (one GPU): the mixed-precision form on the same 256^3 input; the
-batched ensemble (32 cubes of uneven sizes) in FP64 and mixed precision;
+batched ensemble (32 cubes of uneven sizes) in FP64 and mixed precision,
+against its members stepped one after another and against one cube of the
+same cell count;
 c2_256_curves, both forms over 200 steps of the 256^3 case with the
 PrintStats curves every 10 steps; c3_512, the 512^3 case (Mt 0.5,
 Re_lambda 100, 4 x 10^6 particles) over 500 steps in both forms, with the
@@ -304,6 +306,21 @@ def batched_forms(args, local_rank: int, stream):
             s.close()
         return ph_sum, graph_ms, states
 
+    def same_cells_cube(precision):
+        # one cube holding the ensemble's cell count (the nearest even n), the same form, no particles
+        n_eq = int(round(cells ** (1.0 / 3.0) / 2.0)) * 2
+        P, u, v, w, rho, p = ic.make_field(n_eq, MT, RE, SEED)
+        s = Solver(P, cfl=CFL, device=local_rank, precision=precision)
+        s.set_stream(stream.cuda_stream)
+        s.upload_state(ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, p)))
+        if args.autotune_reps > 0:
+            s.autotune(args.autotune_reps)
+        s.step_timed(args.warmup, False)
+        ph = s.step_timed(steps, False)
+        s.close()
+        return {"n": n_eq, "value": n_eq ** 3 * steps / (eul(ph) * 1e-3) / 1e9,
+                "what": "one cube of the ensemble's cell count, same form"}
+
     out = {}
     ph64, g64, l64, cfg64, W64, tke64 = run_ensemble(0)
     phs, gs, Ws = run_sequential()
@@ -319,6 +336,9 @@ def batched_forms(args, local_rank: int, stream):
         "speedup_vs_sequential_graph": gs / g64,
         "max_rel_l2_vs_single_cubes": max(_rel_l2(a, b) for a, b in zip(W64, Ws)),
         "sweep_shapes": cfg64})
+    eq64 = same_cells_cube(0)
+    out["batched_fp64"]["single_cube_same_cells"] = eq64
+    out["batched_fp64"]["over_single_cube_same_cells"] = out["batched_fp64"]["value"] / eq64["value"]
     del Ws
     phm, gm, lm, cfgm, Wm, tkem = run_ensemble(1)
     out["batched_mixed"] = dict(common, **{
@@ -329,6 +349,9 @@ def batched_forms(args, local_rank: int, stream):
         "max_rel_l2_vs_fp64": max(_rel_l2(a, b) for a, b in zip(Wm, W64)),
         "max_tke_rel_err_vs_fp64": max(abs(a - b) / b for a, b in zip(tkem, tke64)),
         "steps_compared": args.warmup + 2 * steps + 1, "sweep_shapes": cfgm})
+    eqm = same_cells_cube(1)
+    out["batched_mixed"]["single_cube_same_cells"] = eqm
+    out["batched_mixed"]["over_single_cube_same_cells"] = out["batched_mixed"]["value"] / eqm["value"]
     return out
 
 
