@@ -135,7 +135,7 @@ def test_64cube_step_matches_oracle(oracle):
 
 def _analytic_case(n, seed):
     """A smooth random-phase velocity field for any n (odd included; the spectral generator
-    needs even n): the odd grids take the cp.async slab copies instead of tensor-map copies."""
+    needs even n)."""
     rng = np.random.default_rng(seed)
     P = ic.Params(n=n, gam=1.4, den0=1.0, Mt=0.3, Re=30.0, mu0=0.9, p0=86100.0, t0=0.01)
     x = (np.arange(n) + 0.5) * (2 * np.pi / n)
@@ -146,8 +146,11 @@ def _analytic_case(n, seed):
     return P, ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, np.full_like(u, P.p0)))
 
 
-@pytest.mark.parametrize("n", [13, 21])
-def test_odd_grids_match_oracle(oracle, n):
+@pytest.mark.parametrize("n", [13, 21, 8, 10, 18])
+def test_odd_and_small_grids_match_oracle(oracle, n):
+    """Odd n: slabs, z boxes and accumulators by per-element copies.  Even n below or just past one
+    16 x 16 window (8, 10, 18): the tensor-copy paths with boxes and bricks that reach past the
+    grid (elements beyond the tensor not read or written, ghost cells stored back unchanged)."""
     P, W0 = _analytic_case(n, 40 + n)
     p = oracle.params(P, 0.5)
     W = W0.copy()
