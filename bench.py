@@ -48,6 +48,7 @@ sys.path.insert(0, ROOT)
 N_CELLS = 256
 N_PART = 1_000_000
 MT, RE, CFL, SEED = 0.3, 60.0, 0.5, 1234
+PERTURBATION = 1e-7   # relative size of the long runs' FP64 control perturbation
 REF_N = 64                   # reference CPU sample: one 64^3 cube per process
 REF_PART = N_PART * REF_N ** 3 // N_CELLS ** 3   # same particle density
 C3_PART = 4_000_000          # particles of the 512^3 mixed-precision case
@@ -365,7 +366,10 @@ def long_run_pair(n, npart, steps, seed, local_rank, stream, autotune_reps=2, st
     src/update.cpp:135-144, 835-841): per form Gcell-updates/s and particle-steps/s over all steps
     (CUDA events per phase), and the mixed form's errors against the FP64 run: relative L2 of rho,
     rho u, rho v, rho w, rho E and of the velocities u, v, w after the last step, and the largest
-    relative difference of every PrintStats curve over the run."""
+    relative difference of every PrintStats curve over the run.  A control run, the FP64 drop-in
+    from the same field with relative noise of single-precision rounding size, gives the
+    same errors for a difference that no precision choice makes: how far the flow itself grows one.
+    Its noise enters after every step, as the mixed form's rounding does."""
     import numpy as np
     import torch
 
@@ -382,8 +386,23 @@ def long_run_pair(n, npart, steps, seed, local_rank, stream, autotune_reps=2, st
         del u, v, w, rho, p
     pos0 = ic.particles_to_reference_order(ic.make_particles(npart, seed))
     nt = n + 6
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 7)
+
+    def perturb(Wd):
+        # the control's step: the state's interior times (1 + PERTURBATION N(0, 1)), seeded, then the
+        # periodic ghosts rewrapped; on the solver's stream, between two steps
+        with torch.cuda.stream(stream):
+            for q in range(5):
+                Wd[q, 3:n + 3, 3:n + 3, 3:n + 3] *= 1.0 + PERTURBATION * torch.randn(
+                    (n, n, n), generator=g, device=dev, dtype=torch.float64)
+            for ax in (1, 2, 3):
+                Wd.narrow(ax, 0, 3).copy_(Wd.narrow(ax, n, 3))
+                Wd.narrow(ax, n + 3, 3).copy_(Wd.narrow(ax, 3, 3))
+
     out, finals, curves, pos = {}, {}, {}, {}
-    for name, prec in (("fp64", 0), ("mixed", 1)):
+    for name, prec in (("fp64", 0), ("mixed", 1), ("fp64_perturbed", 0)):
         s = Solver(P, cfl=CFL, max_particles=npart, device=local_rank, precision=prec)
         s.set_stream(stream.cuda_stream)
         s.upload_state(W0)
@@ -394,8 +413,13 @@ def long_run_pair(n, npart, steps, seed, local_rank, stream, autotune_reps=2, st
             st = s.print_stats()
             curve.append([st["t_over_t0"]] + [st[k] for k in STAT_KEYS])
             k = min(stats_every, steps - done)
-            for key, v in s.step_timed(k, True).items():
-                ph_sum[key] = ph_sum.get(key, 0.0) + v
+            if name == "fp64_perturbed":
+                for _ in range(k):
+                    s.step(1)
+                    perturb(s.device_state())
+            else:
+                for key, v in s.step_timed(k, True).items():
+                    ph_sum[key] = ph_sum.get(key, 0.0) + v
             done += k
         st = s.print_stats()
         curve.append([st["t_over_t0"]] + [st[k] for k in STAT_KEYS])
@@ -405,6 +429,8 @@ def long_run_pair(n, npart, steps, seed, local_rank, stream, autotune_reps=2, st
         s.close()
         finals[name] = Wf
         curves[name] = np.array(curve)
+        if name == "fp64_perturbed":
+            continue
         eul = ph_sum["sweep_x"] + ph_sum["sweep_y"] + ph_sum["sweep_z"] + ph_sum["halo"]
         part = ph_sum["splines"] + ph_sum["particles"]
         out[name] = {"value": n ** 3 * steps / (eul * 1e-3) / 1e9, "unit": "Gcell-updates/s",
@@ -412,22 +438,30 @@ def long_run_pair(n, npart, steps, seed, local_rank, stream, autotune_reps=2, st
                      "ms_per_step": ph_sum["total"] / steps,
                      "phases_ms_per_step": {k: v / steps for k, v in ph_sum.items()}, "sweep_shapes": cfg}
     del W0
-    a, b = finals["mixed"], finals["fp64"]
     sl = (slice(3, nt - 3),) * 3
 
     def rl2(x, y):
         return float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
 
-    err = {nm: rl2(a[q][sl], b[q][sl]) for q, nm in enumerate(("rho", "rho_u", "rho_v", "rho_w", "rho_E"))}
-    for q, nm in ((1, "u"), (2, "v"), (3, "w")):
-        err[nm] = rl2(a[q][sl] / a[0][sl], b[q][sl] / b[0][sl])
-    del a, b, finals
+    def field_err(a, b):
+        e = {nm: rl2(a[q][sl], b[q][sl]) for q, nm in enumerate(("rho", "rho_u", "rho_v", "rho_w", "rho_E"))}
+        for q, nm in ((1, "u"), (2, "v"), (3, "w")):
+            e[nm] = rl2(a[q][sl] / a[0][sl], b[q][sl] / b[0][sl])
+        return e
+
+    err = field_err(finals["mixed"], finals["fp64"])
+    err_control = field_err(finals["fp64_perturbed"], finals["fp64"])
+    del finals
     torch.cuda.empty_cache()
-    cm, cf = curves["mixed"], curves["fp64"]
-    curve_err = {k: float(np.max(np.abs(cm[:, i + 1] - cf[:, i + 1]) / np.maximum(np.abs(cf[:, i + 1]), 1e-300)))
-                 for i, k in enumerate(STAT_KEYS)}
+    cm, cf, cp = curves["mixed"], curves["fp64"], curves["fp64_perturbed"]
+
+    def curve_errs(c):
+        return {k: float(np.max(np.abs(c[:, i + 1] - cf[:, i + 1]) / np.maximum(np.abs(cf[:, i + 1]), 1e-300)))
+                for i, k in enumerate(STAT_KEYS)}
+
+    curve_err = curve_errs(cm)
     # kinetic-energy decay: TKE(t) / TKE(0) of each run
-    decay_m, decay_f = cm[:, 1] / cm[0, 1], cf[:, 1] / cf[0, 1]
+    decay_m, decay_f, decay_p = cm[:, 1] / cm[0, 1], cf[:, 1] / cf[0, 1], cp[:, 1] / cp[0, 1]
     decay_err = float(np.max(np.abs(decay_m - decay_f) / decay_f))
     dx = 2 * np.pi / n
     fields_max = max(err[k] for k in ("rho", "u", "v", "w", "rho_E"))
@@ -444,6 +478,13 @@ def long_run_pair(n, npart, steps, seed, local_rank, stream, autotune_reps=2, st
             np.floor(pos["mixed"] / dx) == np.floor(pos["fp64"] / dx), axis=1))),
         "bars": {"fields_rel_l2": 1e-5, "tke_decay": 1e-3},
         "within_bars": bool(fields_max < 1e-5 and decay_err < 1e-3),
+        "fp64_perturbed_control": {
+            "what": f"the FP64 drop-in from the same field, its state's interior multiplied by (1 + "
+                    f"{PERTURBATION:g} N(0,1)) after every step (seeded noise of single-precision rounding "
+                    "size, as the mixed form's rounding enters every step), against the unperturbed FP64 run",
+            "rel_l2_vs_fp64": err_control,
+            "curve_max_rel_err_vs_fp64": curve_errs(cp),
+            "tke_decay_max_rel_err": float(np.max(np.abs(decay_p - decay_f) / decay_f))},
         "curves": {"columns": ["t_over_t0"] + list(STAT_KEYS),
                    "fp64": cf.tolist(), "mixed": cm.tolist()}})
     return out

@@ -94,6 +94,7 @@ class Solver:
             h = C.c_void_p(_member_handle)
         self.h = h
         self.params = params
+        self.device = device
         self.n = params.n
         self.nt = self.L.gkm_nt(h)
         self.spline_mode = spline_mode
@@ -131,6 +132,18 @@ class Solver:
         out = np.empty((5, self.nt, self.nt, self.nt)) if out is None else out
         self._check(self.L.gkm_download_state(self.h, _w5(out)))
         return out
+
+    def device_state(self):
+        """The current state in device memory as a CUDA tensor view (5, nt, nt, nt), no copy
+        (gkm_device_state); valid until the next step, which writes the other buffer."""
+        import torch
+
+        p = C.POINTER(C.c_double)()
+        self._check(self.L.gkm_device_state(self.h, C.byref(p)))
+        view = type("DeviceState", (), {})()
+        view.__cuda_array_interface__ = {"shape": (5, self.nt, self.nt, self.nt), "typestr": "<f8",
+                                         "data": (C.cast(p, C.c_void_p).value, False), "version": 2}
+        return torch.as_tensor(view, device=f"cuda:{self.device}")
 
     def timestep(self) -> float:
         dt = C.c_double()
