@@ -30,6 +30,7 @@ EXPORTS = [
     "gkm_ensemble_sweep_config", "gkm_ensemble_launch_count", "gkm_ensemble_synchronize", "gkm_ensemble_stream",
     "gkm_particle_props", "gkm_particle_stats_compute", "gkm_write_field", "gkm_write_particles", "gkm_write_time",
     "gkm_write_reinit", "gkm_set_pipeline", "gkm_ensemble_segments", "gkm_set_sweep_config",
+    "gkm_ensemble_set_sweep_config",
 ]
 
 PROP_COUNT = 41
@@ -123,6 +124,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     L.gkm_ensemble_autotune.argtypes = [_h, C.c_int32]
     L.gkm_ensemble_sweep_config.argtypes = [_h, C.POINTER(C.c_int32)]
     L.gkm_ensemble_segments.argtypes = [_h, C.POINTER(C.c_int32), C.c_int64]
+    L.gkm_ensemble_set_sweep_config.argtypes = [_h, C.POINTER(C.c_int32)]
     L.gkm_ensemble_launch_count.argtypes = [_h, C.POINTER(C.c_int64)]
     L.gkm_ensemble_synchronize.argtypes = [_h]
     L.gkm_ensemble_stream.argtypes = [_h, C.POINTER(C.c_void_p)]

@@ -416,7 +416,8 @@ gkm_status gkm_ensemble_autotune(gkm_ensemble* E, int32_t reps)
     };
     const std::vector<int> lens = lens_upto(sizes[0]);
     // the persistent kernel has the plain window variants only (variant 2 is single-cube)
-    const int nvar = E->mixed ? gkm::kSweepVariants32 : 2;
+    // FP64: 16 x 8, 16 x 16, and the warp-specialized 16 x 16 form where its kernels are usable
+    const int nvar = E->mixed ? gkm::kSweepVariants32 : (gkm::ensemble_ws_ready() ? 3 : 2);
     const int p = E->mem[0]->parity;
     cudaEvent_t e0, e1;
     ECK(E, cudaEventCreate(&e0));
@@ -484,6 +485,7 @@ gkm_status gkm_ensemble_autotune(gkm_ensemble* E, int32_t reps)
         cudaMemcpyAsync(E->mem[m]->clock, &saved[(size_t)m], sizeof(DevClock), cudaMemcpyHostToDevice, E->stream);
     cudaStreamSynchronize(E->stream);
     if (st != GKM_OK) return st;
+    destroy_graphs(E);   // a variant of the same windows leaves the work offsets, and so the graphs, unchanged
     return refresh(E, true);
 }
 
@@ -498,6 +500,25 @@ gkm_status gkm_ensemble_segments(const gkm_ensemble* E, int32_t* out, int64_t ca
             out[(size_t)d * nm + m] = L > n ? n : L;
         }
     return GKM_OK;
+}
+
+gkm_status gkm_ensemble_set_sweep_config(gkm_ensemble* E, const int32_t in[6])
+{
+    if (!E || !in) return GKM_ERR_ARG;
+    const int nm = nm_of(E);
+    const int nvar = E->mixed ? gkm::kSweepVariants32 : (gkm::ensemble_ws_ready() ? 3 : 2);
+    for (int d = 0; d < 3; d++) {
+        const int v = in[2 * d], L = in[2 * d + 1];
+        if (L < 1) return efail(E, GKM_ERR_ARG, "segment length below 1");
+        if (v < 0 || v >= nvar) return efail(E, GKM_ERR_CONFIG, "sweep variant not available for this ensemble");
+    }
+    for (int d = 0; d < 3; d++) {
+        E->sweep[d].variant = in[2 * d];
+        E->sweep[d].seg_len = in[2 * d + 1];
+        E->seg[d].assign((size_t)nm, in[2 * d + 1]);
+    }
+    destroy_graphs(E);   // the captured steps launched the previous kernels
+    return refresh(E, false);
 }
 
 gkm_status gkm_ensemble_sweep_config(const gkm_ensemble* E, int32_t out[12])

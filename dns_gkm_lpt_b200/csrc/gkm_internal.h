@@ -58,7 +58,8 @@ using SweepTile64b = SweepTile<16, 16, 1>;
 // FP32: 16 x 8 (168 registers, three CTAs per SM)
 using SweepTile32a = SweepTile<16, 8, 3>;
 // variant 2: 16 x 16 windows, warp-specialized (a producer warpgroup reconstructs face f+1 while
-// two consumer warpgroups compute the fluxes of face f; sweep_ws.cuh), single cubes only
+// two consumer warpgroups compute the fluxes of face f; sweep_ws.cuh); ensembles: its persistent
+// form for x and y
 constexpr int kSweepVariants64 = 3;
 constexpr int kSweepVariants32 = 1;
 
@@ -92,7 +93,8 @@ struct SweepArgs {
 
 // kernel launchers (sweep.cu); sweep_prepare sets the sweep kernels' shared-memory limit once
 cudaError_t sweep_prepare();
-bool ws_ready();   // the warp-specialized FP64 sweep (variant 2) may run
+bool ws_ready();            // the warp-specialized FP64 sweep (variant 2) may run
+bool ensemble_ws_ready();   // and its persistent ensemble form (x, y)
 cudaError_t launch_sweep(int dir, int variant, const SweepArgs& a, int nseg, cudaStream_t s);
 // The sweep of direction dir restricted to the interior y-planes [j0, j1): window rows (x, z
 // sweeps; j0 must be a multiple of the window height) or normal segments from j0 to j1 (y sweep).

@@ -152,6 +152,19 @@ cudaError_t ws_check(bool& ok)
                                 (int)sweep_ws_detail::ws_smem_bytes<SweepTile64b>());
 }
 
+// the persistent ensemble form (x, y): the same register count check, its own shared-memory limit
+template <int DIR>
+cudaError_t ens_ws_check(bool& ok)
+{
+    cudaFuncAttributes at;
+    cudaError_t e = cudaFuncGetAttributes(&at, ensemble_ws_kernel<DIR, SweepTile64b>);
+    if (e != cudaSuccess) return e;
+    ok = ok && at.numRegs == 168;
+    return cudaFuncSetAttribute(ensemble_ws_kernel<DIR, SweepTile64b>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sweep_ws_detail::ws_smem_bytes<SweepTile64b>());
+}
+bool g_ens_ws_ready = false;
+
 // x, y: the form with tensor copies when the launch carries a map; z: per-element copies
 template <int DIR>
 cudaError_t launch_ws(SweepArgs a, dim3 grid, cudaStream_t s)
@@ -223,16 +236,32 @@ cudaError_t sweep_prepare()
     if (e == cudaSuccess) e = ws_check<1, kMapsOff>(ok);
     if (e == cudaSuccess) e = ws_check<2, kMapsOff>(ok);
     g_ws_ready = e == cudaSuccess && ok;
+    bool ens_ok = g_ws_ready;
+    if (e == cudaSuccess) e = ens_ws_check<0>(ens_ok);
+    if (e == cudaSuccess) e = ens_ws_check<1>(ens_ok);
+    g_ens_ws_ready = e == cudaSuccess && ens_ok;
     return e;
 }
 
 bool ws_ready() { return g_ws_ready; }
+bool ensemble_ws_ready() { return g_ens_ws_ready; }
 
 cudaError_t launch_ensemble_sweep64(int dir, int variant, const MemberDev* mem, const long long* off,
                                     const long long* order, int nm, int parity, unsigned long long* next,
                                     cudaStream_t s)
 {
-    // the ensemble's persistent kernel has no warp-specialized form: variant 2 runs as variant 1
+    // variant 2: the persistent warp-specialized form for x and y (one CTA per SM); the z sweep, or a
+    // build whose kernels missed the register count, runs it as variant 1
+    if (variant == 2 && dir < 2 && g_ens_ws_ready) {
+        cudaError_t e = cudaMemsetAsync(next, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return e;
+        const size_t smem = sweep_ws_detail::ws_smem_bytes<SweepTile64b>();
+        if (dir == 0)
+            ensemble_ws_kernel<0, SweepTile64b><<<148, sweep_ws_detail::kThreads, smem, s>>>(mem, off, order, nm, parity, next);
+        else
+            ensemble_ws_kernel<1, SweepTile64b><<<148, sweep_ws_detail::kThreads, smem, s>>>(mem, off, order, nm, parity, next);
+        return cudaGetLastError();
+    }
     if (variant >= 1)
         return launch_ensemble_sweep_t<double, SweepTile64b>(dir, mem, off, order, nm, parity, next, s);
     return launch_ensemble_sweep_t<double, SweepTile64a>(dir, mem, off, order, nm, parity, next, s);

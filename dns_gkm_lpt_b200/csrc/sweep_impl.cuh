@@ -922,6 +922,44 @@ cudaError_t set_form_smem()
     return e;
 }
 
+// Work item `item` of an ensemble sweep of direction DIR: the member it belongs to (members in the
+// order order[], items from off[]), its window (bx, by) and segment bz, and the member's sweep
+// arguments.  Tensor maps: 4 per buffer and window variant (x slab, y slab, z brick, z slab box) of
+// the buffer read and, for the z sweep, the buffer written; `variant` 1 = 16 x 16 windows (FP64),
+// 0 = the 16 x 8 windows (FP64 variant 0 and the mixed form).
+template <int DIR>
+__device__ __forceinline__ void ensemble_item(const MemberDev* __restrict__ mem, const long long* __restrict__ off,
+                                              const long long* __restrict__ order, int nm, int parity, long long item,
+                                              int variant, SweepArgs& a, int& bx, int& by, int& bz)
+{
+    const int pos = find_member(off, nm, item);
+    const MemberDev& md = mem[order[pos]];
+    const long long local = item - off[pos];
+    const int nseg = md.nseg[DIR];
+    const int tb = md.tiles_b[DIR];
+    bz = (int)(local % nseg);
+    const long long t = local / nseg;
+    bx = (int)(t % tb);
+    by = (int)(t / tb);
+    const bool maps = md.tmaps != nullptr;
+    a.tmap = maps ? md.tmaps + 128 * ((parity * kSweepVariants64 + variant) * 4 + (DIR == 2 ? 3 : DIR)) : nullptr;
+    a.tmap_acc = (maps && DIR == 2) ? md.tmaps + 128 * (((parity ^ 1) * kSweepVariants64 + variant) * 4 + 2) : nullptr;
+    a.tmap_wb = (maps && DIR == 2) ? md.tmaps + 128 * ((parity * kSweepVariants64 + variant) * 4 + 2) : nullptr;
+    a.tile_a0 = 0;
+    a.f0 = 0;
+    a.f1 = 0;
+    a.skip_clock_init = 0;
+    a.wait_probe = 0;
+    a.W = md.buf[parity];
+    a.A = md.buf[parity ^ 1];
+    a.fc = md.fc;
+    a.clock = md.clock;
+    a.parity = parity;
+    a.dt_fixed_mode = md.dt_fixed_mode;
+    a.dt_fixed = md.dt_fixed;
+    a.seg_len = md.seg_len[DIR];
+}
+
 // Persistent form for an ensemble: a fixed grid of CTAs takes the flattened
 // (member, window, segment) work list of one sweep direction item by item from
 // a global counter, so a CTA that finishes early takes the next item.  Member
@@ -942,37 +980,10 @@ __global__ void __launch_bounds__(Tile::threads, Tile::ctas)
         __syncthreads();
         const long long item = s_item;
         if (item >= total) break;
-        const int pos = find_member(off, nm, item);
-        const MemberDev& md = mem[order[pos]];
-        const int seg_len = md.seg_len[DIR];
-        const long long local = item - off[pos];
-        const int nseg = md.nseg[DIR];
-        const int tb = md.tiles_b[DIR];
-        const int bz = (int)(local % nseg);
-        const long long t = local / nseg;
         SweepArgs a;
-        // the member's tensor maps (4 per buffer and window variant: x slab, y slab, z brick, z slab
-        // box) of the buffer read and, for the z sweep, the buffer written; variant 1 = 16x16 windows
-        // (FP64 only; the mixed form has one window)
-        constexpr int kVariant = (sizeof(T) == 8 && Tile::TA == 16) ? 1 : 0;
-        const bool maps = md.tmaps != nullptr;
-        a.tmap = maps ? md.tmaps + 128 * ((parity * kSweepVariants64 + kVariant) * 4 + (DIR == 2 ? 3 : DIR)) : nullptr;
-        a.tmap_acc = (maps && DIR == 2) ? md.tmaps + 128 * (((parity ^ 1) * kSweepVariants64 + kVariant) * 4 + 2) : nullptr;
-        a.tmap_wb = (maps && DIR == 2) ? md.tmaps + 128 * ((parity * kSweepVariants64 + kVariant) * 4 + 2) : nullptr;
-        a.tile_a0 = 0;
-        a.f0 = 0;
-        a.f1 = 0;
-        a.skip_clock_init = 0;
-        a.wait_probe = 0;
-        a.W = md.buf[parity];
-        a.A = md.buf[parity ^ 1];
-        a.fc = md.fc;
-        a.clock = md.clock;
-        a.parity = parity;
-        a.dt_fixed_mode = md.dt_fixed_mode;
-        a.dt_fixed = md.dt_fixed;
-        a.seg_len = seg_len;
-        sweep_block<DIR, T, Tile>(a, (int)(t % tb), (int)(t / tb), bz, smem_raw);
+        int bx, by, bz;
+        ensemble_item<DIR>(mem, off, order, nm, parity, item, (sizeof(T) == 8 && Tile::TA == 16) ? 1 : 0, a, bx, by, bz);
+        sweep_block<DIR, T, Tile>(a, bx, by, bz, smem_raw);
         __syncthreads();   // the next item reuses the shared-memory ring
     }
 }

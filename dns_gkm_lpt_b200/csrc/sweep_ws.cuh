@@ -65,7 +65,35 @@ __host__ __device__ constexpr size_t ws_smem_bytes()
 
 }  // namespace sweep_ws_detail
 
-template <int DIR, class Tile, int MM>
+// the mbarriers of a warp-specialized CTA (after its ring, reconstruction buffers and staging):
+// [0] slab copies, [1..2] "full", [3..4] "empty"
+template <class Tile>
+__device__ __forceinline__ unsigned ws_bars(unsigned char* smem_raw)
+{
+    using namespace sweep_detail;
+    const double* stage = reinterpret_cast<const double*>(smem_raw + sweep_ring_bytes<double, Tile>() +
+                                                          sizeof(double) * 10 * Tile::WC);
+    return smem_u32(stage + 5 * sweep_ws_detail::kConsumers);
+}
+__device__ __forceinline__ void ws_init_bars(unsigned bar_tma)
+{
+    using namespace sweep_ws_detail;
+    mbar_init_count(bar_tma, 1);
+    for (int b = 0; b < 2; b++) {
+        mbar_init_count(bar_tma + 8 + 8 * b, kProducers);
+        mbar_init_count(bar_tma + 24 + 8 * b, kConsumers);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void ws_inval_bars(unsigned bar_tma)
+{
+    for (int b = 0; b < 5; b++) asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar_tma + 8 * b) : "memory");
+}
+
+// ROLE 0: the whole CTA (the single-cube kernel: barrier set-up, the register split, both warpgroup
+// roles, barrier retirement).  ROLE 1 / 2: only the producer / consumer part of one work item, for a
+// persistent kernel whose warpgroups have split their registers once and set up the barriers.
+template <int DIR, class Tile, int MM, int ROLE = 0>
 __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int by, int bz, unsigned char* smem_raw)
 {
     using namespace sweep_detail;
@@ -100,24 +128,20 @@ __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int b
     if (f_begin >= f_end) return;
 
     const bool use_tma = DIR != 2 && (MM == kMapsOn || (MM == kMapsRuntime && a.tmap != nullptr));
-    if (tid == 0) {
-        mbar_init_count(bar_tma, 1);
-        for (int b = 0; b < 2; b++) {
-            mbar_init_count(bar_full0 + 8 * b, kProducers);
-            mbar_init_count(bar_empty0 + 8 * b, kConsumers);
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    if constexpr (ROLE == 0) {
+        if (tid == 0) ws_init_bars(bar_tma);
+        __syncthreads();
     }
-    __syncthreads();
 
     auto slot = [&](int f) { return ring + ((f + 12) % kRing) * kSlot; };
     auto recb = [&](int k) { return rec0 + (k & 1) * (10 * kWC); };   // face f_begin - 1 + k
     const int nf = f_end - f_begin + 1;                                   // faces f_begin-1 .. f_end-1
     bool timed_out = false;
 
-    if (tid >= kConsumers) {
+    if (ROLE == 1 || (ROLE == 0 && tid >= kConsumers)) {
+      if constexpr (ROLE != 2) {
         // ------------------------------------------------------------------ producer
-        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kProducerRegs));
+        if constexpr (ROLE == 0) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kProducerRegs));
         const int ptid = tid - kConsumers;
         const bool probe = use_tma && a.wait_probe && bx == 0 && by == 0 && bz == 0;
         unsigned tma_phase = 0;
@@ -240,9 +264,11 @@ __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int b
             }
         }
         if (timed_out) atomicOr(&a.clock->status, 2);
+      }
     } else {
+      if constexpr (ROLE != 1) {
         // ------------------------------------------------------------------ consumers
-        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kConsumerRegs));
+        if constexpr (ROLE == 0) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kConsumerRegs));
         const int tx = tid % kTB, ty = tid / kTB;
         const bool active = (a0 + ty < n) && (b0 + tx < n);
         const int cc = (ty + 1) * kWB + (tx + 1);
@@ -332,10 +358,12 @@ __device__ __forceinline__ void sweep_block_ws(const SweepArgs& a, int bx, int b
             if (bad) atomicOr(&a.clock->status, 1);
         }
         if (timed_out) atomicOr(&a.clock->status, 2);
+      }
     }
-    __syncthreads();   // every wait has returned: retire the barriers
-    if (tid == 0)
-        for (int b = 0; b < 5; b++) asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar_tma + 8 * b) : "memory");
+    if constexpr (ROLE == 0) {
+        __syncthreads();   // every wait has returned: retire the barriers
+        if (tid == 0) ws_inval_bars(bar_tma);
+    }
 }
 
 // MM: compiled for tensor copies of the slabs (x, y sweeps with maps) or per-element copies
@@ -344,6 +372,55 @@ __global__ void __launch_bounds__(sweep_ws_detail::kThreads, 1) sweep_ws_kernel(
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     sweep_block_ws<DIR, Tile, MM>(a, blockIdx.x, blockIdx.y + a.tile_a0, blockIdx.z, smem_raw);
+}
+
+// Persistent warp-specialized form for an ensemble (x, y sweeps, 16 x 16 windows): one CTA per SM takes
+// (member, window, segment) items from the work counter as ensemble_sweep_kernel does.  Each warpgroup
+// splits its registers once and then runs its own loop over the items, so no code is shared between
+// the two register budgets; per item, consumer thread 0 takes the item and sets up fresh barriers,
+// a CTA barrier publishes both, and a second one closes the item.
+template <int DIR, class Tile>
+__global__ void __launch_bounds__(sweep_ws_detail::kThreads, 1)
+    ensemble_ws_kernel(const MemberDev* __restrict__ mem, const long long* __restrict__ off,
+                       const long long* __restrict__ order, int nm, int parity, unsigned long long* next)
+{
+    using namespace sweep_ws_detail;
+    static_assert(DIR != 2, "the z sweep's persistent ensemble form is the plain kernel");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ long long s_item;
+    const long long total = off[nm];
+    const unsigned bars = ws_bars<Tile>(smem_raw);
+    if (threadIdx.x >= kConsumers) {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kProducerRegs));
+        for (;;) {
+            __syncthreads();   // the item and its barriers are set
+            const long long item = s_item;
+            if (item >= total) break;
+            SweepArgs a;
+            int bx, by, bz;
+            ensemble_item<DIR>(mem, off, order, nm, parity, item, 1, a, bx, by, bz);
+            sweep_block_ws<DIR, Tile, kMapsRuntime, 1>(a, bx, by, bz, smem_raw);
+            __syncthreads();   // the item is done
+        }
+    } else {
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kConsumerRegs));
+        for (;;) {
+            if (threadIdx.x == 0) {
+                s_item = (long long)atomicAdd(next, 1ull);
+                ws_init_bars(bars);
+            }
+            __syncthreads();
+            const long long item = s_item;
+            if (item >= total) break;
+            SweepArgs a;
+            int bx, by, bz;
+            ensemble_item<DIR>(mem, off, order, nm, parity, item, 1, a, bx, by, bz);
+            sweep_block_ws<DIR, Tile, kMapsRuntime, 2>(a, bx, by, bz, smem_raw);
+            __syncthreads();
+            if (threadIdx.x == 0) ws_inval_bars(bars);   // every wait of the item has returned
+        }
+        if (threadIdx.x == 0) ws_inval_bars(bars);
+    }
 }
 
 }  // namespace gkm

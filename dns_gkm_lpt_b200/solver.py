@@ -360,6 +360,11 @@ class Ensemble:
                         "segment": out[4 * d + 3], "segment_by_grid_size": dict(sorted(by_n.items()))})
         return cfg
 
+    def set_sweep_config(self, shapes) -> None:
+        """shapes: three (window variant, segment length) pairs for x, y, z, one length for every member."""
+        arr = (C.c_int32 * 6)(*[int(x) for pair in shapes for x in pair])
+        self._check(self.L.gkm_ensemble_set_sweep_config(self.h, arr))
+
     def segments(self) -> list:
         """Segment length of every member, per sweep direction: [x list, y list, z list]."""
         nm = len(self)

@@ -192,8 +192,9 @@ gkm_status gkm_autotune(gkm_handle* h, int32_t reps);
  * window height, segment length (faces per CTA along the normal).  FP64 window
  * variants: 0 = 16 x 8 (two CTAs per SM), 1 = 16 x 16, 2 = 16 x 16
  * warp-specialized (a producer warpgroup reconstructs the next face plane while
- * two consumer warpgroups compute fluxes; single cubes; the plug-point pipeline
- * of gkm_evolve runs it as variant 1).  FP32: 0 = 16 x 8. */
+ * two consumer warpgroups compute fluxes; ensembles run its persistent form for
+ * x and y; the plug-point pipeline of gkm_evolve runs it as variant 1).
+ * FP32: 0 = 16 x 8. */
 gkm_status gkm_sweep_config(const gkm_handle* h, int32_t out[12]);
 /* Set the sweep shapes (no reference counterpart): for x, y, z in turn the
  * window variant and the segment length (in[2d], in[2d+1]).  GKM_ERR_CONFIG for
@@ -372,6 +373,12 @@ gkm_status gkm_ensemble_sweep_config(const gkm_ensemble* e, int32_t out[12]);
 /* Segment length of every member per direction: out[d * n_members + m]
  * (capacity >= 3 x n_members).  No reference counterpart. */
 gkm_status gkm_ensemble_segments(const gkm_ensemble* e, int32_t* out, int64_t capacity);
+/* Set the ensemble's sweep shapes by hand (no reference counterpart): for x, y, z in turn the window
+ * variant and one segment length for every member (in[2d], in[2d+1]); lengths above a member's n
+ * mean one segment.  FP64 variant 2 (16 x 16, warp-specialized) runs the persistent
+ * warp-specialized kernel for x and y and the 16 x 16 kernel for z.  GKM_ERR_CONFIG for a variant
+ * this precision or this GPU does not have. */
+gkm_status gkm_ensemble_set_sweep_config(gkm_ensemble* e, const int32_t in[6]);
 gkm_status gkm_ensemble_launch_count(const gkm_ensemble* e, int64_t* count);
 gkm_status gkm_ensemble_synchronize(gkm_ensemble* e);
 /* The ensemble's stream (cudaStream_t as void*), for events or interop. */

@@ -177,3 +177,38 @@ def test_ensemble_eulerian_only_equals_evolve_eulerian():
         E.step(4, with_particles=False)
         for m in range(len(specs)):
             assert rel_l2(E[m].download_state(), single[m]).max() <= 1e-13
+
+
+def test_ensemble_warp_specialized_sweeps_match_single_cubes():
+    """Window variant 2 in the ensemble: the persistent warp-specialized kernel for x and y (each
+    warpgroup looping over the work items with its own register budget), 16 x 16 windows for z; the
+    members must match single cubes stepped with the warp-specialized sweeps (bitwise where the
+    arithmetic is the same; the single cubes' z sweep is the warp-specialized kernel there, so
+    within rounding) and the plain ensemble."""
+    members = [{"params": _member_inputs(s)[0], "cfl": 0.5, "max_particles": s[4]} for s in RAGGED]
+    out = {}
+    for var in (1, 2):
+        with Ensemble(members) as E:
+            E.set_sweep_config([(var, 16)] * 3)
+            assert [c["variant"] for c in E.sweep_config()] == [var] * 3
+            for m, spec in enumerate(RAGGED):
+                _, W0, pos = _member_inputs(spec)
+                E[m].upload_state(W0)
+                if pos is not None:
+                    E[m].particles_upload(pos)
+            E.step(5)
+            out[var] = [_outputs(E[m], spec[4]) for m, spec in enumerate(RAGGED)]
+    _compare(out[2], out[1], 1e-14, 1e-12, "FP64 ensemble variant 2 vs variant 1")
+    single = []
+    for spec in RAGGED:
+        P, W0, pos = _member_inputs(spec)
+        with Solver(P, cfl=0.5, max_particles=spec[4]) as s:
+            s.set_sweep_config([(2, 16)] * 3)
+            s.upload_state(W0)
+            if pos is not None:
+                s.particles_upload(pos)
+            s.step(5)
+            single.append(_outputs(s, spec[4]))
+    _compare(out[2], single, 1e-14, 1e-12, "FP64 ensemble variant 2 vs single cubes variant 2")
+    with Ensemble(members[:1]) as E, pytest.raises(GkmError):
+        E.set_sweep_config([(3, 16)] * 3)
