@@ -400,6 +400,12 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
     const T eps_T = kMixed ? T(fc.eps_T) : T(kWenoEps);
     const double* __restrict__ W = a.W;
     const double suth_c = fc.mu0 * (fc.T0 + 110.4) * kR / ((kR * fc.T0) * sqrt(kR * fc.T0));
+    // mixed form: tau' = tau us / dx = tc_a x^(3/2) / ((x + tc_b) p') (Sutherland) or tc_a x^0.76 / p'
+    // (power law), x = T / T0, p' = p / p0
+    const float tc_a = kMixed ? float(fc.visc == 1 ? fc.mu0 * fc.u_s * fc.inv_dx / fc.p0
+                                                   : fc.mu0 * (fc.T0 + 110.4) * fc.u_s * fc.inv_dx / (fc.T0 * fc.p0))
+                              : 0.f;
+    const float tc_b = kMixed ? float(110.4 / fc.T0) : 0.f;
 
     if (DIR == 0 && bx == 0 && by == 0 && bz == 0 && tid == 0 && !a.skip_clock_init) {
         a.clock->wave[a.parity ^ 1] = 0ull;   // the z sweep of this step reduces into it
@@ -789,8 +795,9 @@ __device__ __forceinline__ void sweep_block(const SweepArgs& a, int bx, int by, 
                 const float d = wl[cc], id = 1.0f / d;
                 const float u = wl[kWC + cc] * id, v = wl[2 * kWC + cc] * id, w = wl[3 * kWC + cc] * id;
                 const float p = (d * float(fc.gm1)) * (wl[4 * kWC + cc] * id - 0.5f * (u * u + v * v + w * w));
-                const double Tk = (double)(p * id) * fc.T0;
-                tau0 = T(collision_time(fc, Tk, (double)p * fc.p0) * fc.u_s * fc.inv_dx);
+                const float x = p * id;   // T / T0
+                // mu(T) / p in the working units, in single precision like the flux it enters
+                tau0 = fc.visc == 1 ? tc_a * powf(x, 0.76f) / p : tc_a * (x * sqrtf(x)) / ((x + tc_b) * p);
             } else if (fc.visc == 1) {
                 double d = wl[cc], id = 1.0 / d;
                 double u = wl[kWC + cc] * id, v = wl[2 * kWC + cc] * id, w = wl[3 * kWC + cc] * id;
