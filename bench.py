@@ -27,8 +27,10 @@ mixed form's field and curve errors against the FP64 run.
 --impl reference: the reference's own CPU code (oracle/_ref, compiled from
 the reference sources) on all host cores, one 64^3 cube per process (the
 per-cell rate stands in for the 256^3 cube: extrapolated), all processes
-concurrent, --warmup untimed and --steps timed reference steps each.  The
-GPU arm's cpu_baseline is the same measurement.
+concurrent, --warmup untimed and --steps timed reference steps each.  Where
+that build is absent, the oracle's C restatement of the Eulerian step runs
+instead ("kind": "port").  The GPU arm's cpu_baseline is the same
+measurement.
 """
 from __future__ import annotations
 
@@ -172,14 +174,34 @@ class ClockSampler:
 
 
 # ------------------------------------------------------- reference arm ----
+def _reference_built() -> bool:
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    return os.path.exists(O.REF_SO)
+
+
 def _ref_worker(args):
-    """One process: the reference CPU build on one seeded REF_N^3 cube."""
+    """One process: the reference CPU build on one seeded REF_N^3 cube, or, where that build is
+    absent, the oracle's C restatement of the Eulerian step (no particles) on the same cube."""
     n, npart, seed, warm, steps = args
     sys.path.insert(0, ROOT)
     from dns_gkm_lpt_b200 import ic
     from oracle import oracle as O
-    d = tempfile.mkdtemp(prefix="gkm_ref_")
     P, u, v, w, rho, p = ic.make_field(n, MT, RE, seed)
+    if not os.path.exists(O.REF_SO):
+        orc = O.Oracle()
+        W = ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, p))
+        par = orc.params(P, CFL)
+
+        def one():
+            t = time.perf_counter()
+            orc.step(par, W, orc.timestep(par, W))
+            return time.perf_counter() - t, 0.0
+
+        for _ in range(warm):
+            one()
+        return [one() for _ in range(steps)]
+    d = tempfile.mkdtemp(prefix="gkm_ref_")
     ic.write_reference_inputs(d, P, u, v, w, rho, p, ic.make_particles(npart, seed))
     ref = O.ReferenceRun(d, CFL, True)
     if warm:
@@ -188,6 +210,7 @@ def _ref_worker(args):
 
 
 def run_reference(workers: int, warm: int, steps: int, n=REF_N, npart=REF_PART):
+    kind = "reference" if _reference_built() else "port"
     ctx = mp.get_context("spawn")
     t0 = time.time()
     with ctx.Pool(workers) as pool:
@@ -198,13 +221,16 @@ def run_reference(workers: int, warm: int, steps: int, n=REF_N, npart=REF_PART):
     gcell = sum(n ** 3 * steps / t for t in te) / 1e9
     psteps = sum(npart * steps / t for t in tp) if all(t > 0 for t in tp) else None
     ms_step = 1e3 * statistics.mean([(a + b) / steps for a, b in zip(te, tp)])
-    return {"gcell": gcell, "psteps": psteps, "ms_per_step": ms_step, "workers": workers, "wall_s": wall}
+    return {"gcell": gcell, "psteps": psteps, "ms_per_step": ms_step, "workers": workers, "wall_s": wall,
+            "kind": kind}
 
 
-def reference_sample_text(workers, warm, steps, wall_s):
+def reference_sample_text(workers, warm, steps, wall_s, kind="reference"):
+    what = ("timed reference steps each" if kind == "reference" else
+            "timed Eulerian steps each of the oracle's C restatement (the reference build was absent)")
     return (f"{REF_N}^3 cube per process (same spectrum recipe, Mt {MT}, Re_lambda {RE:g}), {REF_PART} particles "
             f"per process (the 256^3 case's particle density), {workers} concurrent single-rank processes on "
-            f"{workers} host cores, {warm} warm-up + {steps} timed reference steps each ({wall_s:.1f} s wall); "
+            f"{workers} host cores, {warm} warm-up + {steps} {what} ({wall_s:.1f} s wall); "
             f"Gcell-updates/s is the per-cell rate of those cubes, standing in for the 256^3 cube "
             f"(extrapolated: a 256^3 step takes ~2 min on one core, and the reference parallelises only "
             f"through MPI, which this box lacks)")
@@ -227,8 +253,8 @@ def reference_arm(args, world: int):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded solenoidal field (init_DNS recipe), uniform particles",
             "config": reference_config(workers), "particle_steps_per_s": r["psteps"],
-            "cpu_baseline": {"value": r["gcell"], "unit": "Gcell-updates/s", "cores": workers, "kind": "reference",
-                             "sample": reference_sample_text(workers, args.warmup, args.steps, r["wall_s"])},
+            "cpu_baseline": {"value": r["gcell"], "unit": "Gcell-updates/s", "cores": workers, "kind": r["kind"],
+                             "sample": reference_sample_text(workers, args.warmup, args.steps, r["wall_s"], r["kind"])},
             "e2e": {"value": r["gcell"], "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -693,8 +719,8 @@ def ours(args, rank: int, world: int, local_rank: int):
         workers = max(1, min(os.cpu_count() or 1, 96))
         r = run_reference(workers, args.warmup, args.steps)
         line["cpu_baseline"] = {"value": r["gcell"], "unit": "Gcell-updates/s", "cores": workers,
-                                "kind": "reference",
-                                "sample": reference_sample_text(workers, args.warmup, args.steps, r["wall_s"]),
+                                "kind": r["kind"],
+                                "sample": reference_sample_text(workers, args.warmup, args.steps, r["wall_s"], r["kind"]),
                                 "particle_steps_per_s": r["psteps"]}
     print(json.dumps(line), flush=True)
 
