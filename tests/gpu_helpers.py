@@ -25,3 +25,16 @@ def rel_l2(a, b):
 def case(n, Mt, Re, seed):
     P, u, v, w, rho, p = ic.make_field(n, Mt, Re, seed)
     return P, ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, p))
+
+
+def analytic_case(n, seed):
+    """A smooth random-phase velocity field for any n (odd included; the spectral generator
+    needs even n)."""
+    rng = np.random.default_rng(seed)
+    P = ic.Params(n=n, gam=1.4, den0=1.0, Mt=0.3, Re=30.0, mu0=0.9, p0=86100.0, t0=0.01)
+    x = (np.arange(n) + 0.5) * (2 * np.pi / n)
+    Y, X, Z = np.meshgrid(x, x, x, indexing="ij")
+    u, v, w = [sum(rng.uniform(20, 60) * np.sin(kx * X + ky * Y + kz * Z + rng.uniform(0, 2 * np.pi))
+                   for kx, ky, kz in ((1, 0, 1), (0, 2, 1), (1, 1, 0))) for _ in range(3)]
+    rho = 1.0 + 0.05 * np.cos(X + 2 * Z)
+    return P, ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, np.full_like(u, P.p0)))

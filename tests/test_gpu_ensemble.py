@@ -24,7 +24,7 @@ import pytest
 
 from dns_gkm_lpt_b200 import ic
 from dns_gkm_lpt_b200.solver import Ensemble, GkmError, Solver
-from tests.gpu_helpers import case, rel_l2, w0_of
+from tests.gpu_helpers import analytic_case, case, rel_l2, w0_of
 
 pytestmark = pytest.mark.gpu
 
@@ -212,3 +212,27 @@ def test_ensemble_warp_specialized_sweeps_match_single_cubes():
     _compare(out[2], single, 1e-14, 1e-12, "FP64 ensemble variant 2 vs single cubes variant 2")
     with Ensemble(members[:1]) as E, pytest.raises(GkmError):
         E.set_sweep_config([(3, 16)] * 3)
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_ensemble_with_odd_grid_members_matches_single_cubes(variant):
+    """Odd n gives an odd extent nt, so those members have no tensor maps: their work items take
+    the per-element copies inside the same persistent launches whose other items use tensor copies
+    (the plain kernel for variant 1; for variant 2 the warp-specialized x and y kernel, whose
+    producer and consumer warpgroups decide per item)."""
+    cases = [analytic_case(13, 61), case(16, 0.3, 40.0, 62), analytic_case(21, 63), case(24, 0.4, 30.0, 64)]
+    single = []
+    for P, W0 in cases:
+        with Solver(P, cfl=0.5) as s:
+            s.set_sweep_config([(variant, 16)] * 3)
+            s.upload_state(W0)
+            s.evolve_eulerian(4)
+            single.append(s.download_state())
+    with Ensemble([{"params": P, "cfl": 0.5} for P, _ in cases]) as E:
+        E.set_sweep_config([(variant, 16)] * 3)
+        for m, (_, W0) in enumerate(cases):
+            E[m].upload_state(W0)
+        E.step(4, with_particles=False)
+        for m in range(len(cases)):
+            assert rel_l2(E[m].download_state(), single[m]).max() <= 1e-13, m
+

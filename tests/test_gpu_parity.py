@@ -15,7 +15,7 @@ import pytest
 
 from dns_gkm_lpt_b200 import ic
 from dns_gkm_lpt_b200.solver import GkmError, Solver, flux_faces, weno_faces
-from tests.gpu_helpers import case, params_of, rel_l2, w0_of
+from tests.gpu_helpers import analytic_case, case, params_of, rel_l2, w0_of
 
 pytestmark = pytest.mark.gpu
 
@@ -133,25 +133,12 @@ def test_64cube_step_matches_oracle(oracle):
         assert rel_l2(s.download_state(), Wo).max() <= FIELD_TOL
 
 
-def _analytic_case(n, seed):
-    """A smooth random-phase velocity field for any n (odd included; the spectral generator
-    needs even n)."""
-    rng = np.random.default_rng(seed)
-    P = ic.Params(n=n, gam=1.4, den0=1.0, Mt=0.3, Re=30.0, mu0=0.9, p0=86100.0, t0=0.01)
-    x = (np.arange(n) + 0.5) * (2 * np.pi / n)
-    Y, X, Z = np.meshgrid(x, x, x, indexing="ij")
-    u, v, w = [sum(rng.uniform(20, 60) * np.sin(kx * X + ky * Y + kz * Z + rng.uniform(0, 2 * np.pi))
-                   for kx, ky, kz in ((1, 0, 1), (0, 2, 1), (1, 1, 0))) for _ in range(3)]
-    rho = 1.0 + 0.05 * np.cos(X + 2 * Z)
-    return P, ic.embed_ghost(ic.primitive_to_conserved(P, u, v, w, rho, np.full_like(u, P.p0)))
-
-
 @pytest.mark.parametrize("n", [13, 21, 8, 10, 18])
 def test_odd_and_small_grids_match_oracle(oracle, n):
     """Odd n: slabs, z boxes and accumulators by per-element copies.  Even n below or just past one
     16 x 16 window (8, 10, 18): the tensor-copy paths with boxes and bricks that reach past the
     grid (elements beyond the tensor not read or written, ghost cells stored back unchanged)."""
-    P, W0 = _analytic_case(n, 40 + n)
+    P, W0 = analytic_case(n, 40 + n)
     p = oracle.params(P, 0.5)
     W = W0.copy()
     r = oracle.run(p, W, 3, 0, None, stats=False)
