@@ -214,25 +214,25 @@ def test_ensemble_warp_specialized_sweeps_match_single_cubes():
         E.set_sweep_config([(3, 16)] * 3)
 
 
-@pytest.mark.parametrize("variant", [1, 2])
-def test_ensemble_with_odd_grid_members_matches_single_cubes(variant):
+@pytest.mark.parametrize("precision,variant,tol", [(0, 1, 1e-13), (0, 2, 1e-13), (1, 0, 1e-6)])
+def test_ensemble_with_odd_grid_members_matches_single_cubes(precision, variant, tol):
     """Odd n gives an odd extent nt, so those members have no tensor maps: their work items take
     the per-element copies inside the same persistent launches whose other items use tensor copies
-    (the plain kernel for variant 1; for variant 2 the warp-specialized x and y kernel, whose
-    producer and consumer warpgroups decide per item)."""
+    (FP64: the plain kernel for variant 1; for variant 2 the warp-specialized x and y kernel, whose
+    producer and consumer warpgroups decide per item; mixed: its one window variant)."""
     cases = [analytic_case(13, 61), case(16, 0.3, 40.0, 62), analytic_case(21, 63), case(24, 0.4, 30.0, 64)]
     single = []
     for P, W0 in cases:
-        with Solver(P, cfl=0.5) as s:
+        with Solver(P, cfl=0.5, precision=precision) as s:
             s.set_sweep_config([(variant, 16)] * 3)
             s.upload_state(W0)
             s.evolve_eulerian(4)
             single.append(s.download_state())
-    with Ensemble([{"params": P, "cfl": 0.5} for P, _ in cases]) as E:
+    with Ensemble([{"params": P, "cfl": 0.5} for P, _ in cases], precision=precision) as E:
         E.set_sweep_config([(variant, 16)] * 3)
         for m, (_, W0) in enumerate(cases):
             E[m].upload_state(W0)
         E.step(4, with_particles=False)
         for m in range(len(cases)):
-            assert rel_l2(E[m].download_state(), single[m]).max() <= 1e-13, m
+            assert rel_l2(E[m].download_state(), single[m]).max() <= tol, m
 
