@@ -103,6 +103,26 @@ def test_spline_coefficients_bitexact_with_oracle(oracle, golden, mode, build):
         assert np.array_equal(got[c], ref), c
 
 
+@pytest.mark.parametrize("build", [1, 2])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_spline_coefficients_bitexact_on_an_odd_grid(oracle, mode, build):
+    """n = 13: lines of 19 (natural) or 13 (periodic) points, an odd count of both lines and
+    points per line, in both launch forms."""
+    P, W0 = analytic_case(13, 5)
+    p = oracle.params(P, 0.5)
+    start, dinv = oracle.grid(p, mode)
+    with Solver(P, cfl=0.5, spline_mode=mode, spline_build=build) as s:
+        s.upload_state(W0)
+        s.generate_splines()
+        got = [s.spline_coefs(c) for c in range(3)]
+    for c in range(3):
+        data = W0[1 + c] / W0[0]
+        if mode == 1:
+            data = np.ascontiguousarray(data[3:-3, 3:-3, 3:-3])
+        _, ref = oracle.spline3d(data, mode, start, dinv)
+        assert np.array_equal(got[c], ref), c
+
+
 @pytest.mark.parametrize("mode", [0, 1])
 def test_particles_match_oracle_both_spline_modes(oracle, mode):
     P, W0 = case(16, 0.4, 40.0, 31)
