@@ -287,122 +287,130 @@ __global__ void spline_pass1(const double* __restrict__ in, SplineGrid g, Spline
 constexpr int kLineChunk = 32;
 constexpr int kPass2Warps = 4;
 
-// lines [L0, L0 + 32) of a pass-2 input (lines total), by one warp with its staging rows sm
+// lines [L0, L0 + 32) of a pass-2 input (lines total), by one warp with its staging rows sm.
+// Chunks are 32 output slots [s0, s0 + 32), holding values s0 - 1 .. s0 + 30 of the line (value i
+// lands in slot i + 1): the copies out, and the backward sweep's copies back in, then cover whole
+// 32-byte sectors of the output rows (2,112 bytes, a multiple of 32) instead of starting 8 bytes
+// into one.
 __device__ __forceinline__ void pass2_group(const double* __restrict__ in, const SplineGrid& g, const SplineTables& tb,
                                             double* __restrict__ out, long long L0, long long lines,
                                             double (*sm)[kLineChunk + 1])
 {
     const int N = g.npts, M = N + g.pad;
     const int lane = threadIdx.x & 31;
-    {
-        const int nl = (int)min(32LL, lines - L0);           // lines of this warp
-        const long long myL = L0 + lane;
-        const bool mine = lane < nl;
-        // load chunk [k0, k0+kLineChunk) of the warp's lines into sm[j][t]
-        auto load = [&](const double* base, long long stride, int k0, int off) {
-            for (int j = 0; j < nl; j++) {
-                const int k = k0 + lane;
-                if (k < N) sm[j][lane] = base[(L0 + j) * stride + k + off];
-            }
-            __syncwarp();
-        };
-        auto store = [&](double* base, long long stride, int k0, int off, int kmax) {
-            __syncwarp();
-            for (int j = 0; j < nl; j++) {
-                const int k = k0 + lane;
-                if (k < kmax) base[(L0 + j) * stride + k + off] = sm[j][lane];
-            }
-            __syncwarp();
-        };
-        const double* src = in + myL * N;
-        double* dst = out + myL * M;
-        if (!g.periodic) {
-            const double c0 = mine ? src[0] : 0.0, cl = mine ? src[N - 1] : 0.0;
-            // forward elimination: slot i+1 <- rp_i for i = 1..N-2 (chunks of i)
-            double rp = 0.0;
-            for (int k0 = 0; k0 < N; k0 += kLineChunk) {
-                load(in, N, k0, 0);
-                if (mine)
-                    for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
-                        const int i = k0 + t;
-                        if (i < 1 || i > N - 2) continue;
-                        double r = mul(6.0, sm[lane][t]);
-                        if (i == 1) r = sub(r, c0);
-                        if (i == N - 2) r = sub(r, cl);
-                        rp = (i == 1) ? r : sub(r, mul(tb.mt[i], rp));
-                        sm[lane][t] = rp;
-                    }
-                store(out, M, k0, 1, N);   // value of i lands in slot i+1
-            }
-            // back substitution, chunks in descending order
-            double x = 0.0, x1 = 0.0, xl2 = 0.0;
-            for (int k0 = ((N - 1) / kLineChunk) * kLineChunk; k0 >= 0; k0 -= kLineChunk) {
-                load(out, M, k0, 1);
-                if (mine)
-                    for (int t = kLineChunk - 1; t >= 0; t--) {
-                        const int i = k0 + t;
-                        if (i < 1 || i > N - 2) continue;
-                        x = (i == N - 2) ? __ddiv_rn(sm[lane][t], tb.dp[N - 2])
-                                         : __ddiv_rn(sub(sm[lane][t], x), tb.dp[i]);
-                        sm[lane][t] = x;
-                        if (i == N - 2) xl2 = x;
-                        if (i == 1) x1 = x;
-                    }
-                store(out, M, k0, 1, N);
-            }
-            if (mine) {
-                dst[1] = c0;
-                dst[N] = cl;
-                dst[0] = sub(2.0 * c0, x1);
-                dst[N + 1] = sub(2.0 * cl, xl2);
-            }
-        } else {
-            double rp = 0.0;
-            for (int k0 = 0; k0 < N; k0 += kLineChunk) {
-                load(in, N, k0, 0);
-                if (mine)
-                    for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
-                        const int i = k0 + t;
-                        rp = (i == 0) ? mul(6.0, sm[lane][t]) : sub(mul(6.0, sm[lane][t]), mul(tb.mt[i], rp));
-                        sm[lane][t] = rp;
-                    }
-                store(out, M, k0, 1, N);
-            }
-            double x = 0.0, x0 = 0.0, xl = 0.0;
-            for (int k0 = ((N - 1) / kLineChunk) * kLineChunk; k0 >= 0; k0 -= kLineChunk) {
-                load(out, M, k0, 1);
-                if (mine)
-                    for (int t = kLineChunk - 1; t >= 0; t--) {
-                        const int i = k0 + t;
-                        if (i > N - 1) continue;
-                        x = (i == N - 1) ? __ddiv_rn(sm[lane][t], tb.dp[N - 1])
-                                         : __ddiv_rn(sub(sm[lane][t], x), tb.dp[i]);
-                        sm[lane][t] = x;
-                        if (i == N - 1) xl = x;
-                        if (i == 0) x0 = x;
-                    }
-                store(out, M, k0, 1, N);
-            }
-            const double fac = mine ? __ddiv_rn(add(x0, mul(-0.25, xl)), tb.denom) : 0.0;
-            double y0 = 0.0, y1 = 0.0, yl = 0.0;
-            for (int k0 = 0; k0 < N; k0 += kLineChunk) {
-                load(out, M, k0, 1);
-                if (mine)
-                    for (int t = 0; t < kLineChunk && k0 + t < N; t++) {
-                        const int i = k0 + t;
-                        const double v = sub(sm[lane][t], mul(fac, tb.z[i]));
-                        sm[lane][t] = v;
-                        if (i == 0) y0 = v;
-                        if (i == 1) y1 = v;
-                        if (i == N - 1) yl = v;
-                    }
-                store(out, M, k0, 1, N);
-            }
-            if (mine) {
-                dst[0] = yl;
-                dst[N + 1] = y0;
-                dst[N + 2] = y1;
-            }
+    const int nl = (int)min(32LL, lines - L0);   // lines of this warp
+    const long long myL = L0 + lane;
+    const bool mine = lane < nl;
+    // values s0 - 1 + lane of the warp's lines from the input rows (N values each)
+    auto load_in = [&](int s0) {
+        const int e = s0 - 1 + lane;
+        if (e >= 0 && e < N)
+            for (int j = 0; j < nl; j++) sm[j][lane] = in[(L0 + j) * N + e];
+        __syncwarp();
+    };
+    // slots s0 + lane (1..N) of the warp's output rows, in and out
+    auto load_out = [&](int s0) {
+        const int sl = s0 + lane;
+        if (sl >= 1 && sl <= N)
+            for (int j = 0; j < nl; j++) sm[j][lane] = out[(L0 + j) * M + sl];
+        __syncwarp();
+    };
+    auto store_out = [&](int s0) {
+        __syncwarp();
+        const int sl = s0 + lane;
+        if (sl >= 1 && sl <= N)
+            for (int j = 0; j < nl; j++) out[(L0 + j) * M + sl] = sm[j][lane];
+        __syncwarp();
+    };
+    const int s_last = (N / kLineChunk) * kLineChunk;   // the chunk holding slot N
+    const double* src = in + myL * N;
+    double* dst = out + myL * M;
+    if (!g.periodic) {
+        const double c0 = mine ? src[0] : 0.0, cl = mine ? src[N - 1] : 0.0;
+        // forward elimination: slot i+1 <- rp_i for i = 1..N-2 (values 0 and N-1 land in slots 1, N)
+        double rp = 0.0;
+        for (int s0 = 0; s0 <= s_last; s0 += kLineChunk) {
+            load_in(s0);
+            if (mine)
+                for (int t = 0; t < kLineChunk; t++) {
+                    const int i = s0 - 1 + t;
+                    if (i < 1 || i > N - 2) continue;
+                    double r = mul(6.0, sm[lane][t]);
+                    if (i == 1) r = sub(r, c0);
+                    if (i == N - 2) r = sub(r, cl);
+                    rp = (i == 1) ? r : sub(r, mul(tb.mt[i], rp));
+                    sm[lane][t] = rp;
+                }
+            store_out(s0);
+        }
+        // back substitution, chunks in descending order
+        double x = 0.0, x1 = 0.0, xl2 = 0.0;
+        for (int s0 = s_last; s0 >= 0; s0 -= kLineChunk) {
+            load_out(s0);
+            if (mine)
+                for (int t = kLineChunk - 1; t >= 0; t--) {
+                    const int i = s0 - 1 + t;
+                    if (i < 1 || i > N - 2) continue;
+                    x = (i == N - 2) ? __ddiv_rn(sm[lane][t], tb.dp[N - 2]) : __ddiv_rn(sub(sm[lane][t], x), tb.dp[i]);
+                    sm[lane][t] = x;
+                    if (i == N - 2) xl2 = x;
+                    if (i == 1) x1 = x;
+                }
+            store_out(s0);
+        }
+        if (mine) {
+            dst[1] = c0;
+            dst[N] = cl;
+            dst[0] = sub(2.0 * c0, x1);
+            dst[N + 1] = sub(2.0 * cl, xl2);
+        }
+    } else {
+        double rp = 0.0;
+        for (int s0 = 0; s0 <= s_last; s0 += kLineChunk) {
+            load_in(s0);
+            if (mine)
+                for (int t = 0; t < kLineChunk; t++) {
+                    const int i = s0 - 1 + t;
+                    if (i < 0 || i > N - 1) continue;
+                    rp = (i == 0) ? mul(6.0, sm[lane][t]) : sub(mul(6.0, sm[lane][t]), mul(tb.mt[i], rp));
+                    sm[lane][t] = rp;
+                }
+            store_out(s0);
+        }
+        double x = 0.0, x0 = 0.0, xl = 0.0;
+        for (int s0 = s_last; s0 >= 0; s0 -= kLineChunk) {
+            load_out(s0);
+            if (mine)
+                for (int t = kLineChunk - 1; t >= 0; t--) {
+                    const int i = s0 - 1 + t;
+                    if (i < 0 || i > N - 1) continue;
+                    x = (i == N - 1) ? __ddiv_rn(sm[lane][t], tb.dp[N - 1]) : __ddiv_rn(sub(sm[lane][t], x), tb.dp[i]);
+                    sm[lane][t] = x;
+                    if (i == N - 1) xl = x;
+                    if (i == 0) x0 = x;
+                }
+            store_out(s0);
+        }
+        const double fac = mine ? __ddiv_rn(add(x0, mul(-0.25, xl)), tb.denom) : 0.0;
+        double y0 = 0.0, y1 = 0.0, yl = 0.0;
+        for (int s0 = 0; s0 <= s_last; s0 += kLineChunk) {
+            load_out(s0);
+            if (mine)
+                for (int t = 0; t < kLineChunk; t++) {
+                    const int i = s0 - 1 + t;
+                    if (i < 0 || i > N - 1) continue;
+                    const double v = sub(sm[lane][t], mul(fac, tb.z[i]));
+                    sm[lane][t] = v;
+                    if (i == 0) y0 = v;
+                    if (i == 1) y1 = v;
+                    if (i == N - 1) yl = v;
+                }
+            store_out(s0);
+        }
+        if (mine) {
+            dst[0] = yl;
+            dst[N + 1] = y0;
+            dst[N + 2] = y1;
         }
     }
 }
